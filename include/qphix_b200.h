@@ -1,0 +1,323 @@
+/*
+ * qphix_b200.h -- C-ABI of the B200 (sm_100a) dslash library.
+ *
+ * The library computes the operator family that qphix-codegen emits for CPU
+ * ISAs: the Wilson, clover, twisted-mass (TM) and twisted-mass-clover
+ * hopping terms, in the plain "dslash" form and in the "achimbdpsi" form
+ * (A.chi - b.D.psi), for isign = +1 ("plus") and -1 ("minus", the dagger),
+ * with 18-real or 12-real (two stored rows) gauge links and twisted boundary
+ * phases, plus the halo (face) pack and unpack kernels.
+ *
+ * Every field lives in device memory in the QPhiX tile layouts of
+ * codegen/include/decl_common.h:9-62 (Types<FT,V,S,compress12>):
+ *   spinor  FourSpinorBlock  FT[3 colour][4 spin][2 re/im][S]       per S x-sites
+ *   gauge   SU3MatrixBlock   FT[8 dir][2|3 row][3][2][V]            per tile of V sites
+ *   clover  CloverBlock      {diag1[6][V]; off_diag1[15][2][V];
+ *                             diag2[6][V]; off_diag2[15][2][V]}       per tile
+ *   tmclov  FullCloverBlock  {block1[6][6][2][V]; block2[6][6][2][V]} per tile
+ * A tile covers V/S consecutive y rows of S x-sites each.  The reference
+ * kernels work on one tile per call and leave the lattice loop, neighbour
+ * offsets and per-tile boundary coefficients to the caller (QPhiX); here one
+ * call covers a whole checkerboard of a (sub-)lattice described by
+ * qb200_lattice, and the neighbour addressing is computed on the device.
+ *
+ * Conventions (all taken from the reference generator):
+ *   - dir d = 2*mu + {0 back, 1 forw}, mu = x,y,z,t   (codegen/dslash.cc:232-233)
+ *   - stored link matrix G = U^T: forward hop uses sum_k G[k][c] b[k], backward
+ *     hop sum_k conj(G[c][k]) b[k]  (codegen/dslash_common.cc:1678-1727)
+ *   - 12-real links rebuild G[2][c] = conj(G[0][c+1]G[1][c+2]-G[0][c+2]G[1][c+1])
+ *     (codegen/dslash_common.cc:1657-1676)
+ *   - "half" storage is IEEE binary16 bits with no scale (decl_common.h:7)
+ *
+ * Layout of one site (xcb, y, z, t) on checkerboard cb (x = 2*xcb + ((y+z+t+cb)&1)):
+ *   nxh = nx/2, nvecs = nxh/S, ngy = V/S
+ *   Pxy  = ny*nvecs + pad_xy,  Pxyz = nz*Pxy + pad_xyz
+ *   spinor block  = t*Pxyz + z*Pxy + y*nvecs + xcb/S,      lane = xcb%S
+ *   gauge/clover tile = ((t*nz + z)*(ny/ngy) + y/ngy)*nvecs + xcb/S,
+ *                 lane = (y%ngy)*S + xcb%S
+ *   spinor field length = nt*Pxyz blocks; gauge/clover length = nt*nz*(ny/ngy)*nvecs tiles
+ *
+ * Face (halo) buffers are site-major: FT[n_face_sites][2 spin][3 colour][2 re/im],
+ * the half-spinor ordering of codegen/data_types.cc:508-543 with one site per
+ * entry.  Face sites are enumerated in increasing (t, z, y, xcb) order of the
+ * sites whose coordinate in the face dimension is 0 (back face) or N-1
+ * (forward face).
+ *
+ * Error convention: every entry point returns QB200_OK (0) or a negative
+ * QB200_E* code and never aborts the process (the reference prints and calls
+ * exit(1) on a bad dir, codegen/jinja/dslash_spec.h.j2:28-31).
+ * qb200_last_error() returns a message for the calling thread's last error.
+ *
+ * Streams: `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ * stream).  Calls are asynchronous with respect to the host; the library
+ * allocates no device memory on these paths.
+ */
+#ifndef QPHIX_B200_H
+#define QPHIX_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QB200_ABI_VERSION 1
+
+/* status codes */
+#define QB200_OK 0
+#define QB200_EINVAL (-1)   /* bad scalar argument or lattice description */
+#define QB200_ENULL (-2)    /* a required pointer is NULL */
+#define QB200_ELAYOUT (-3)  /* (ftype, soalen, veclen) combination not built */
+#define QB200_EDIR (-4)     /* dir outside 0..7 */
+#define QB200_ECUDA (-5)    /* CUDA launch or runtime error */
+#define QB200_EALIGN (-6)   /* device pointer not aligned to the block size */
+#define QB200_ENODEV (-7)   /* no CUDA device */
+
+/* storage types (FT of the reference templates) */
+#define QB200_F32 0
+#define QB200_F64 1
+#define QB200_F16 2 /* IEEE binary16 bits, unscaled: the reference's `half` */
+
+typedef struct qb200_lattice {
+  int nx, ny, nz, nt; /* local lattice extents in full sites; nx even */
+  int soalen;         /* S: x-sites per spinor block (1,2,4,8,16) */
+  int veclen;         /* V: sites per gauge/clover tile; V % S == 0 */
+  int pad_xy;         /* spinor blocks of padding after each xy plane */
+  int pad_xyz;        /* spinor blocks of padding after each xyz volume */
+  int ftype;          /* QB200_F32 / QB200_F64 / QB200_F16 */
+  int compress12;     /* 1: gauge tiles store 2 rows (12 reals), 0: 3 rows */
+  /* time boundary: hops that cross the global t edge are multiplied by
+   * t_boundary (+1 periodic, -1 antiperiodic).  t_edge_lo / t_edge_hi say
+   * whether local t = 0 / t = nt-1 lie on the global edge (1 on one GPU). */
+  double t_boundary;
+  int t_edge_lo, t_edge_hi;
+} qb200_lattice;
+
+/* ---- library information --------------------------------------------- */
+int qb200_abi_version(void);
+const char *qb200_last_error(void);
+/* 1 if the (ftype, soalen) pair has compiled kernels, else 0 */
+int qb200_layout_supported(int ftype, int soalen);
+/* number of elements (FT units) of one checkerboard field */
+long long qb200_spinor_elems(const qb200_lattice *lat);
+long long qb200_gauge_elems(const qb200_lattice *lat);
+long long qb200_clover_elems(const qb200_lattice *lat);
+long long qb200_full_clover_elems(const qb200_lattice *lat);
+/* number of sites on face `dir` (0..7) of one checkerboard */
+long long qb200_face_sites(const qb200_lattice *lat, int dir);
+
+/*
+ * ---- body kernels ------------------------------------------------------
+ * Common arguments:
+ *   cb          checkerboard of `out` (and chi); psi lives on 1-cb
+ *   accumulate  8 flags.  accumulate[d] != 0: every hop in direction d is
+ *               added.  accumulate[d] == 0: hops in direction d that leave
+ *               the local sub-lattice are skipped; face_*finish_dir adds them
+ *               later.  (The reference passes these per tile; QPhiX clears
+ *               them only on tiles at a communicated boundary.)  NULL = all on.
+ *   coeff_s     hop coefficient for x, y, z;  coeff_t_f / coeff_t_b for
+ *               forward / backward t hops (codegen/dslash.cc:79-86)
+ *   tbc_mask    bit mu set: twisted boundary phase tbc_phases[mu] multiplies
+ *               every forward hop in dim mu, its conjugate every backward hop
+ *               (the tbc_x..tbc_t template flags; dslash_common.cc:1491-1524)
+ *   tbc_phases  [4][2] (re, im); may be NULL when tbc_mask == 0
+ */
+
+/* Wilson: out = D psi.  Replaces QPhiX::dslash_{plus,minus}_vec
+ * (codegen/jinja/dslash_decl.h.j2:6-43). */
+int qb200_dslash_plus_vec(const qb200_lattice *lat, int cb, const void *psi,
+                          void *out, const void *gauge,
+                          const unsigned accumulate[8], double coeff_s,
+                          double coeff_t_f, double coeff_t_b,
+                          unsigned tbc_mask, const double *tbc_phases,
+                          void *stream);
+int qb200_dslash_minus_vec(const qb200_lattice *lat, int cb, const void *psi,
+                           void *out, const void *gauge,
+                           const unsigned accumulate[8], double coeff_s,
+                           double coeff_t_f, double coeff_t_b,
+                           unsigned tbc_mask, const double *tbc_phases,
+                           void *stream);
+
+/* Wilson: out = alpha chi - D psi (hops subtracted).  Replaces
+ * QPhiX::dslash_achimbdpsi_{plus,minus}_vec (dslash_decl.h.j2:45-88). */
+int qb200_dslash_achimbdpsi_plus_vec(
+    const qb200_lattice *lat, int cb, const void *psi, const void *chi,
+    void *out, const void *gauge, double alpha, double coeff_s,
+    double coeff_t_f, double coeff_t_b, unsigned tbc_mask,
+    const double *tbc_phases, const unsigned accumulate[8], void *stream);
+int qb200_dslash_achimbdpsi_minus_vec(
+    const qb200_lattice *lat, int cb, const void *psi, const void *chi,
+    void *out, const void *gauge, double alpha, double coeff_s,
+    double coeff_t_f, double coeff_t_b, unsigned tbc_mask,
+    const double *tbc_phases, const unsigned accumulate[8], void *stream);
+
+/* Clover: out = A (D psi), A a Hermitian CloverBlock field (callers pass
+ * A^-1 for the even-odd operator).  Replaces
+ * QPhiX::clov_dslash_{plus,minus}_vec (clov_dslash_decl.h.j2:5-46). */
+int qb200_clov_dslash_plus_vec(const qb200_lattice *lat, int cb,
+                               const void *psi, void *out, const void *gauge,
+                               const void *clover,
+                               const unsigned accumulate[8], double coeff_s,
+                               double coeff_t_f, double coeff_t_b,
+                               unsigned tbc_mask, const double *tbc_phases,
+                               void *stream);
+int qb200_clov_dslash_minus_vec(const qb200_lattice *lat, int cb,
+                                const void *psi, void *out,
+                                const void *gauge, const void *clover,
+                                const unsigned accumulate[8], double coeff_s,
+                                double coeff_t_f, double coeff_t_b,
+                                unsigned tbc_mask, const double *tbc_phases,
+                                void *stream);
+
+/* Clover: out = A chi + i rho g5 chi (sign flips for minus) - D psi.
+ * Replaces QPhiX::clov_dslash_achimbdpsi_{plus,minus}_vec
+ * (clov_dslash_decl.h.j2:48-94; dslash_common.cc:1830-1932). */
+int qb200_clov_dslash_achimbdpsi_plus_vec(
+    const qb200_lattice *lat, int cb, const void *psi, const void *chi,
+    void *out, const void *gauge, const void *clover, double coeff_s,
+    double coeff_t_f, double coeff_t_b, unsigned tbc_mask,
+    const double *tbc_phases, const unsigned accumulate[8],
+    double prec_mass_rho, void *stream);
+int qb200_clov_dslash_achimbdpsi_minus_vec(
+    const qb200_lattice *lat, int cb, const void *psi, const void *chi,
+    void *out, const void *gauge, const void *clover, double coeff_s,
+    double coeff_t_f, double coeff_t_b, unsigned tbc_mask,
+    const double *tbc_phases, const unsigned accumulate[8],
+    double prec_mass_rho, void *stream);
+
+/* Twisted mass: out = muinv (1 -/+ i mu g5) D psi.  Replaces
+ * QPhiX::tm_dslash_{plus,minus}_vec (tm_dslash_decl.h.j2:5-45;
+ * inverse_twisted_term, dslash_common.cc:1234-1359). */
+int qb200_tm_dslash_plus_vec(const qb200_lattice *lat, int cb,
+                             const void *psi, void *out, const void *gauge,
+                             const unsigned accumulate[8], double coeff_s,
+                             double coeff_t_f, double coeff_t_b,
+                             unsigned tbc_mask, const double *tbc_phases,
+                             double mu, double muinv, void *stream);
+int qb200_tm_dslash_minus_vec(const qb200_lattice *lat, int cb,
+                              const void *psi, void *out, const void *gauge,
+                              const unsigned accumulate[8], double coeff_s,
+                              double coeff_t_f, double coeff_t_b,
+                              unsigned tbc_mask, const double *tbc_phases,
+                              double mu, double muinv, void *stream);
+
+/* Twisted mass: out = alpha (1 +/- i mu g5) chi - D psi.  Replaces
+ * QPhiX::tm_dslash_achimbdpsi_{plus,minus}_vec (tm_dslash_decl.h.j2:47-91;
+ * twisted_term, dslash_common.cc:1364-1489). */
+int qb200_tm_dslash_achimbdpsi_plus_vec(
+    const qb200_lattice *lat, int cb, const void *psi, const void *chi,
+    void *out, const void *gauge, double alpha, double coeff_s,
+    double coeff_t_f, double coeff_t_b, unsigned tbc_mask,
+    const double *tbc_phases, double mu, const unsigned accumulate[8],
+    void *stream);
+int qb200_tm_dslash_achimbdpsi_minus_vec(
+    const qb200_lattice *lat, int cb, const void *psi, const void *chi,
+    void *out, const void *gauge, double alpha, double coeff_s,
+    double coeff_t_f, double coeff_t_b, unsigned tbc_mask,
+    const double *tbc_phases, double mu, const unsigned accumulate[8],
+    void *stream);
+
+/* Twisted-mass clover: out = F (D psi), F a dense FullCloverBlock field.
+ * Replaces QPhiX::tm_clov_dslash_{plus,minus}_vec
+ * (tm_clov_dslash_decl.h.j2; full_clover_term, dslash_common.cc:1188-1232). */
+int qb200_tm_clov_dslash_plus_vec(const qb200_lattice *lat, int cb,
+                                  const void *psi, void *out,
+                                  const void *gauge, const void *full_clover,
+                                  const unsigned accumulate[8],
+                                  double coeff_s, double coeff_t_f,
+                                  double coeff_t_b, unsigned tbc_mask,
+                                  const double *tbc_phases, void *stream);
+int qb200_tm_clov_dslash_minus_vec(const qb200_lattice *lat, int cb,
+                                   const void *psi, void *out,
+                                   const void *gauge, const void *full_clover,
+                                   const unsigned accumulate[8],
+                                   double coeff_s, double coeff_t_f,
+                                   double coeff_t_b, unsigned tbc_mask,
+                                   const double *tbc_phases, void *stream);
+
+/* Twisted-mass clover: out = F chi + i rho g5 chi - D psi.  Replaces
+ * QPhiX::tm_clov_dslash_achimbdpsi_{plus,minus}_vec
+ * (tm_clov_dslash_decl.h.j2:48-94). */
+int qb200_tm_clov_dslash_achimbdpsi_plus_vec(
+    const qb200_lattice *lat, int cb, const void *psi, const void *chi,
+    void *out, const void *gauge, const void *full_clover, double coeff_s,
+    double coeff_t_f, double coeff_t_b, unsigned tbc_mask,
+    const double *tbc_phases, const unsigned accumulate[8],
+    double prec_mass_rho, void *stream);
+int qb200_tm_clov_dslash_achimbdpsi_minus_vec(
+    const qb200_lattice *lat, int cb, const void *psi, const void *chi,
+    void *out, const void *gauge, const void *full_clover, double coeff_s,
+    double coeff_t_f, double coeff_t_b, unsigned tbc_mask,
+    const double *tbc_phases, const unsigned accumulate[8],
+    double prec_mass_rho, void *stream);
+
+/*
+ * ---- face (halo) kernels -----------------------------------------------
+ * face_proj_dir: project the sites of `psi` (checkerboard psi_cb) that lie on
+ * the face towards `dir` with the projector of the opposite direction and
+ * write them to outbuf (the neighbour in direction dir needs them).
+ * Replaces QPhiX::face_proj_dir_{plus,minus} (dslash_decl.h.j2:90-99;
+ * pack_face_vec, dslash.cc:433-458).
+ */
+int qb200_face_proj_dir_plus(const qb200_lattice *lat, int psi_cb,
+                             const void *psi, void *outbuf, int dir,
+                             void *stream);
+int qb200_face_proj_dir_minus(const qb200_lattice *lat, int psi_cb,
+                              const void *psi, void *outbuf, int dir,
+                              void *stream);
+
+/*
+ * face_*finish_dir: for the output sites (checkerboard cb) on the face of
+ * `dir`, multiply the received half spinors by the link of direction dir,
+ * reconstruct and accumulate into out (read-modify-write).  Wilson and TM
+ * faces subtract beta*hop, clover and TM-clover faces add beta*hop and apply
+ * the clover field to it (codegen/dslash_common.cc:1934-1993).  tbc != 0
+ * applies tbc_phases[dir/2].  Replaces QPhiX::face_finish_dir_*,
+ * face_clov_finish_dir_*, tm_face_finish_dir_*, tm_clov_face_finish_dir_*
+ * (dslash_decl.h.j2:101-115, clov_dslash_decl.h.j2:214-231,
+ * tm_dslash_decl.h.j2:93-109, tm_clov_dslash_decl.h.j2:97-113).
+ */
+int qb200_face_finish_dir_plus(const qb200_lattice *lat, int cb,
+                               const void *inbuf, const void *gauge,
+                               void *out, double beta, int dir, int tbc,
+                               const double *tbc_phases, void *stream);
+int qb200_face_finish_dir_minus(const qb200_lattice *lat, int cb,
+                                const void *inbuf, const void *gauge,
+                                void *out, double beta, int dir, int tbc,
+                                const double *tbc_phases, void *stream);
+int qb200_face_clov_finish_dir_plus(const qb200_lattice *lat, int cb,
+                                    const void *inbuf, const void *gauge,
+                                    void *out, const void *clover,
+                                    double beta, int dir, int tbc,
+                                    const double *tbc_phases, void *stream);
+int qb200_face_clov_finish_dir_minus(const qb200_lattice *lat, int cb,
+                                     const void *inbuf, const void *gauge,
+                                     void *out, const void *clover,
+                                     double beta, int dir, int tbc,
+                                     const double *tbc_phases, void *stream);
+int qb200_tm_face_finish_dir_plus(const qb200_lattice *lat, int cb,
+                                  const void *inbuf, const void *gauge,
+                                  void *out, double beta, double mu,
+                                  double muinv, int dir, int tbc,
+                                  const double *tbc_phases, void *stream);
+int qb200_tm_face_finish_dir_minus(const qb200_lattice *lat, int cb,
+                                   const void *inbuf, const void *gauge,
+                                   void *out, double beta, double mu,
+                                   double muinv, int dir, int tbc,
+                                   const double *tbc_phases, void *stream);
+int qb200_tm_clov_face_finish_dir_plus(const qb200_lattice *lat, int cb,
+                                       const void *inbuf, const void *gauge,
+                                       void *out, const void *full_clover,
+                                       double beta, int dir, int tbc,
+                                       const double *tbc_phases,
+                                       void *stream);
+int qb200_tm_clov_face_finish_dir_minus(const qb200_lattice *lat, int cb,
+                                        const void *inbuf, const void *gauge,
+                                        void *out, const void *full_clover,
+                                        double beta, int dir, int tbc,
+                                        const double *tbc_phases,
+                                        void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QPHIX_B200_H */

@@ -1,0 +1,91 @@
+#!/usr/bin/env python3
+"""Build libqphix_b200.so in-tree for sm_100a with nvcc.
+
+The body and face kernels are instantiated once per (storage type, SOALEN)
+from csrc/qb200_inst.cu so that the objects compile in parallel; the C-ABI
+layer is csrc/qb200_api.cu.  Objects go to qphix-codegen_b200/_build/, the
+library to qphix-codegen_b200/qphix_b200/libqphix_b200.so.
+Usage: python qphix-codegen_b200/build.py [-j N] [--force]
+"""
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "qphix_b200", "libqphix_b200.so")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
+           "-Xptxas", "-v", "--expt-relaxed-constexpr", "-I" + CSRC, "-I" + INCLUDE]
+
+FTYPES = {"f32": "float", "f64": "double", "f16": "__half"}
+SOALENS = [1, 2, 4, 8, 16]
+
+
+def nvcc():
+    p = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(p):
+        raise RuntimeError("nvcc not found")
+    return p
+
+
+def units():
+    """(object path, extra flags, source) for every translation unit."""
+    out = [(os.path.join(BUILD, "qb200_api.o"), [], os.path.join(CSRC, "qb200_api.cu"))]
+    for tag, ft in FTYPES.items():
+        for s in SOALENS:
+            out.append((os.path.join(BUILD, "inst_%s_s%d.o" % (tag, s)),
+                        ["-DQB_FT=%s" % ft, "-DQB_S=%d" % s],
+                        os.path.join(CSRC, "qb200_inst.cu")))
+    return out
+
+
+def newest_source():
+    return max(os.path.getmtime(os.path.join(d, f))
+               for d in (CSRC, INCLUDE) for f in os.listdir(d))
+
+
+def compile_one(obj, extra, src, log):
+    cmd = [nvcc()] + ARCH + NVFLAGS + extra + ["-c", src, "-o", obj]
+    r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    with open(log, "w") as f:
+        f.write(" ".join(cmd) + "\n" + r.stdout)
+    if r.returncode:
+        raise RuntimeError("nvcc failed for %s:\n%s" % (obj, r.stdout[-6000:]))
+    return obj
+
+
+def build(jobs=None, force=False, verbose=True):
+    os.makedirs(BUILD, exist_ok=True)
+    src_t = newest_source()
+    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= src_t:
+        return LIB
+    jobs = jobs or max(1, os.cpu_count() or 1)
+    todo = []
+    for obj, extra, src in units():
+        if force or not os.path.exists(obj) or os.path.getmtime(obj) < src_t:
+            todo.append((obj, extra, src, obj + ".log"))
+    with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
+        futs = [ex.submit(compile_one, *t) for t in todo]
+        for fu in cf.as_completed(futs):
+            o = fu.result()
+            if verbose:
+                print("built", os.path.relpath(o, HERE), flush=True)
+    objs = [u[0] for u in units()]
+    cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+    r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if r.returncode:
+        raise RuntimeError("link failed:\n" + r.stdout[-4000:])
+    return LIB
+
+
+if __name__ == "__main__":
+    j = None
+    if "-j" in sys.argv:
+        j = int(sys.argv[sys.argv.index("-j") + 1])
+    print(build(jobs=j, force="--force" in sys.argv))

@@ -1,0 +1,123 @@
+// qb200_inst.cu -- kernel instantiations and launchers for one storage type
+// and SOALEN.  Compiled once per (QB_FT, QB_S) pair by the build so that the
+// translation units build in parallel.
+#include "qb200_face_kernel.cuh"
+#include "qb200_internal.h"
+
+#ifndef QB_FT
+#error "QB_FT (float, double, __half) must be defined"
+#endif
+#ifndef QB_S
+#error "QB_S (SOALEN) must be defined"
+#endif
+
+namespace qb200 {
+
+namespace {
+constexpr int kThreads = 128;
+
+template <typename FT, int S, bool COMP12, int FAM, bool ACH>
+cudaError_t go(const KArgs<FT> &a, const GeoDev &g, const OpDev<typename ftraits<FT>::C> &p,
+               cudaStream_t st)
+{
+  const int blocks = (g.nsites + kThreads - 1) / kThreads;
+  site_dslash_kernel<FT, S, COMP12, FAM, ACH><<<blocks, kThreads, 0, st>>>(a, g, p);
+  return cudaGetLastError();
+}
+
+template <typename FT, int S, bool COMP12>
+cudaError_t go_fam(const LaunchSpec &ls, const KArgs<FT> &a, const GeoDev &g,
+                   const OpDev<typename ftraits<FT>::C> &p, cudaStream_t st)
+{
+  switch (ls.fam * 2 + (ls.ach ? 1 : 0)) {
+  case 0: return go<FT, S, COMP12, FAM_WILSON, false>(a, g, p, st);
+  case 1: return go<FT, S, COMP12, FAM_WILSON, true>(a, g, p, st);
+  case 2: return go<FT, S, COMP12, FAM_CLOVER, false>(a, g, p, st);
+  case 3: return go<FT, S, COMP12, FAM_CLOVER, true>(a, g, p, st);
+  case 4: return go<FT, S, COMP12, FAM_TM, false>(a, g, p, st);
+  case 5: return go<FT, S, COMP12, FAM_TM, true>(a, g, p, st);
+  case 6: return go<FT, S, COMP12, FAM_TMCLOV, false>(a, g, p, st);
+  case 7: return go<FT, S, COMP12, FAM_TMCLOV, true>(a, g, p, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <typename FT, int S, bool COMP12, int FAM>
+cudaError_t go_unpack(const FT *buf, const FT *gauge, const FT *clov, FT *out, const GeoDev &g,
+                      const FaceDev &f, const OpDev<typename ftraits<FT>::C> &p, cudaStream_t st)
+{
+  const int blocks = (f.nface + kThreads - 1) / kThreads;
+  face_unpack_kernel<FT, S, COMP12, FAM><<<blocks, kThreads, 0, st>>>(buf, gauge, clov, out, g, f, p);
+  return cudaGetLastError();
+}
+
+FaceDev to_dev(const FaceSpec &s)
+{
+  FaceDev f;
+  f.dir = s.dir;
+  f.mu = s.mu;
+  f.coord = s.coord;
+  f.par = s.par;
+  f.nface = s.nface;
+  f.cb = s.cb;
+  return f;
+}
+} // namespace
+
+template <typename FT, int S>
+cudaError_t launch_dslash(const LaunchSpec &ls, const FT *psi, const FT *chi, const FT *gauge,
+                          const FT *clov, FT *out, const GeoDev &g,
+                          const OpDev<typename ftraits<FT>::C> &p, cudaStream_t st)
+{
+  KArgs<FT> a;
+  a.psi = psi;
+  a.chi = chi;
+  a.gauge = gauge;
+  a.clov = clov;
+  a.out = out;
+  if (g.nsites == 0) return cudaSuccess;
+  return ls.comp12 ? go_fam<FT, S, true>(ls, a, g, p, st) : go_fam<FT, S, false>(ls, a, g, p, st);
+}
+
+template <typename FT, int S>
+cudaError_t launch_face_pack(const FT *psi, FT *buf, const GeoDev &g, const FaceSpec &fs, int isPlus,
+                             cudaStream_t st)
+{
+  if (fs.nface == 0) return cudaSuccess;
+  const FaceDev f = to_dev(fs);
+  const int blocks = (f.nface + kThreads - 1) / kThreads;
+  face_pack_kernel<FT, S><<<blocks, kThreads, 0, st>>>(psi, buf, g, f, isPlus);
+  return cudaGetLastError();
+}
+
+template <typename FT, int S>
+cudaError_t launch_face_unpack(int fam, bool comp12, const FT *buf, const FT *gauge, const FT *clov,
+                               FT *out, const GeoDev &g, const FaceSpec &fs,
+                               const OpDev<typename ftraits<FT>::C> &p, cudaStream_t st)
+{
+  if (fs.nface == 0) return cudaSuccess;
+  const FaceDev f = to_dev(fs);
+  switch (fam * 2 + (comp12 ? 1 : 0)) {
+  case 0: return go_unpack<FT, S, false, FAM_WILSON>(buf, gauge, clov, out, g, f, p, st);
+  case 1: return go_unpack<FT, S, true, FAM_WILSON>(buf, gauge, clov, out, g, f, p, st);
+  case 2: return go_unpack<FT, S, false, FAM_CLOVER>(buf, gauge, clov, out, g, f, p, st);
+  case 3: return go_unpack<FT, S, true, FAM_CLOVER>(buf, gauge, clov, out, g, f, p, st);
+  case 4: return go_unpack<FT, S, false, FAM_TM>(buf, gauge, clov, out, g, f, p, st);
+  case 5: return go_unpack<FT, S, true, FAM_TM>(buf, gauge, clov, out, g, f, p, st);
+  case 6: return go_unpack<FT, S, false, FAM_TMCLOV>(buf, gauge, clov, out, g, f, p, st);
+  case 7: return go_unpack<FT, S, true, FAM_TMCLOV>(buf, gauge, clov, out, g, f, p, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template cudaError_t launch_dslash<QB_FT, QB_S>(const LaunchSpec &, const QB_FT *, const QB_FT *,
+                                                const QB_FT *, const QB_FT *, QB_FT *, const GeoDev &,
+                                                const OpDev<ftraits<QB_FT>::C> &, cudaStream_t);
+template cudaError_t launch_face_pack<QB_FT, QB_S>(const QB_FT *, QB_FT *, const GeoDev &,
+                                                   const FaceSpec &, int, cudaStream_t);
+template cudaError_t launch_face_unpack<QB_FT, QB_S>(int, bool, const QB_FT *, const QB_FT *,
+                                                     const QB_FT *, QB_FT *, const GeoDev &,
+                                                     const FaceSpec &, const OpDev<ftraits<QB_FT>::C> &,
+                                                     cudaStream_t);
+
+} // namespace qb200

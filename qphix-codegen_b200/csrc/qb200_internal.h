@@ -1,0 +1,37 @@
+// qb200_internal.h -- host-side declarations shared by the C-ABI layer and
+// the per-(storage type, SOALEN) kernel translation units.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "qb200_device.cuh"
+
+namespace qb200 {
+
+// what one launch computes
+struct LaunchSpec {
+  int fam;        // FAM_WILSON .. FAM_TMCLOV
+  bool ach;       // achimbdpsi form
+  bool comp12;    // 12-real links
+};
+
+// body kernel launcher, defined in qb200_inst.cu for each (FT, S)
+template <typename FT, int S>
+cudaError_t launch_dslash(const LaunchSpec &ls, const FT *psi, const FT *chi, const FT *gauge,
+                          const FT *clov, FT *out, const GeoDev &g,
+                          const OpDev<typename ftraits<FT>::C> &p, cudaStream_t st);
+
+// face launchers, defined in qb200_inst.cu for each (FT, S)
+struct FaceSpec {
+  int dir, mu, coord, par, nface, cb;
+};
+template <typename FT, int S>
+cudaError_t launch_face_pack(const FT *psi, FT *buf, const GeoDev &g, const FaceSpec &f, int isPlus,
+                             cudaStream_t st);
+template <typename FT, int S>
+cudaError_t launch_face_unpack(int fam, bool comp12, const FT *buf, const FT *gauge, const FT *clov,
+                               FT *out, const GeoDev &g, const FaceSpec &f,
+                               const OpDev<typename ftraits<FT>::C> &p, cudaStream_t st);
+
+} // namespace qb200

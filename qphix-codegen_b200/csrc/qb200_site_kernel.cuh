@@ -1,0 +1,153 @@
+// qb200_site_kernel.cuh -- thread-per-site dslash kernel, generic over every
+// QPhiX tile layout (storage type FT, SOALEN S, VECLEN as run-time V).
+//
+// One thread computes one output site of the checkerboard: the eight hops of
+// dslash_body (codegen/dslash.cc:200-323) in registers, followed by the
+// clover / twisted-mass post-term of dslash_plain_body or the A.chi pre-term
+// of dslash_achimbdpsi_body (codegen/dslash_common.cc:1729-1932).
+#pragma once
+
+#include "qb200_device.cuh"
+
+namespace qb200 {
+
+template <typename FT> struct KArgs {
+  const FT *psi;
+  const FT *chi;
+  const FT *gauge;
+  const FT *clov;
+  FT *out;
+};
+
+template <typename FT, int S, bool COMP12, int D>
+__device__ __forceinline__ void do_hop(const KArgs<FT> &a, const GeoDev &g,
+                                       const OpDev<typename ftraits<FT>::C> &p, const Site &s,
+                                       long long gbase,
+                                       cx<typename ftraits<FT>::C> (&acc)[4][3])
+{
+  typedef typename ftraits<FT>::C C;
+  constexpr int MU = D / 2;
+  constexpr bool FWD = (D & 1) != 0;
+  bool cross;
+  const Site n = neighbour<D>(g, s, &cross);
+  if (cross && !((p.acc_mask >> D) & 1u)) return;
+  C beta = p.beta[D];
+  if (D == 6 && s.t == 0 && p.t_edge_lo) beta *= p.tbound;
+  if (D == 7 && s.t == g.nt - 1 && p.t_edge_hi) beta *= p.tbound;
+
+  cx<C> psi[4][3], b[2][3], ub[2][3], G[3][3];
+  load_spinor<FT, S>(a.psi, spinor_base<S>(g, n), psi);
+  const C sigma = p.isPlus ? (C)1 : (C)-1;
+  project<C, D>(psi, sigma, b);
+  load_link<FT, COMP12, D>(a.gauge, gbase, g.V, G);
+  mult_link<C, !FWD>(G, b, ub);
+  if ((p.tbc_mask >> MU) & 1u) {
+    const C pr = p.tbc[MU][0];
+    const C pi = FWD ? p.tbc[MU][1] : -p.tbc[MU][1];
+    apply_phase<C>(ub, pr, pi);
+  }
+  // rec_plus for (isPlus xor fwd)
+  const C tau = ((p.isPlus != 0) != FWD) ? (C)1 : (C)-1;
+  recons<C, MU>(ub, beta, tau, acc);
+}
+
+template <typename FT, int S, bool COMP12, int FAM, bool ACH>
+__global__ void __launch_bounds__(128)
+    site_dslash_kernel(const KArgs<FT> a, const GeoDev g, const OpDev<typename ftraits<FT>::C> p)
+{
+  typedef typename ftraits<FT>::C C;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.nsites) return;
+  const Site s = site_of(g, i, p.cb);
+  int lane;
+  const long long tile = tile_of<S>(g, s, &lane);
+  constexpr int R = COMP12 ? 2 : 3;
+  const long long gbase = tile * (8LL * R * 6 * g.V) + lane;
+  const long long obase = spinor_base<S>(g, s);
+
+  cx<C> res[4][3];
+  cx<C> acc[4][3];
+#pragma unroll
+  for (int sp = 0; sp < 4; sp++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) res[sp][c] = mk<C>(0, 0);
+
+  if (ACH) {
+    // A.chi first (achiResult, dslash_common.cc:1559-1655), then the hops are
+    // subtracted (beta already negated by the host)
+    cx<C> ch[4][3];
+    load_spinor<FT, S>(a.chi, obase, ch);
+    if (FAM == FAM_WILSON) {
+#pragma unroll
+      for (int sp = 0; sp < 4; sp++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) res[sp][c] = mk<C>(p.alpha * ch[sp][c].re, p.alpha * ch[sp][c].im);
+    } else if (FAM == FAM_TM) {
+      // alpha (1 +/- i mu g5) chi, + on the upper spins for plus
+#pragma unroll
+      for (int sp = 0; sp < 4; sp++) {
+        const C m = (((sp < 2) == (p.isPlus != 0)) ? (C)1 : (C)-1) * p.mu;
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+          res[sp][c] = mk<C>(p.alpha * fma(-m, ch[sp][c].im, ch[sp][c].re),
+                             p.alpha * fma(m, ch[sp][c].re, ch[sp][c].im));
+      }
+    } else {
+      const long long cbase = tile * ((FAM == FAM_CLOVER ? 72LL : 144LL) * g.V) + lane;
+#pragma unroll
+      for (int blk = 0; blk < 2; blk++) {
+        if (FAM == FAM_CLOVER) clover_block<FT, false>(a.clov, cbase, g.V, blk, ch, res);
+        else full_clover_block<FT, false>(a.clov, cbase, g.V, blk, ch, res);
+      }
+      // + i rho g5 chi for plus (dslash_common.cc:1873-1906)
+#pragma unroll
+      for (int sp = 0; sp < 4; sp++) {
+        const C r = (((p.isPlus != 0) != (sp >= 2)) ? (C)1 : (C)-1) * p.rho;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          res[sp][c].re = fma(-r, ch[sp][c].im, res[sp][c].re);
+          res[sp][c].im = fma(r, ch[sp][c].re, res[sp][c].im);
+        }
+      }
+    }
+    do_hop<FT, S, COMP12, 0>(a, g, p, s, gbase, res);
+    do_hop<FT, S, COMP12, 1>(a, g, p, s, gbase, res);
+    do_hop<FT, S, COMP12, 2>(a, g, p, s, gbase, res);
+    do_hop<FT, S, COMP12, 3>(a, g, p, s, gbase, res);
+    do_hop<FT, S, COMP12, 4>(a, g, p, s, gbase, res);
+    do_hop<FT, S, COMP12, 5>(a, g, p, s, gbase, res);
+    do_hop<FT, S, COMP12, 6>(a, g, p, s, gbase, res);
+    do_hop<FT, S, COMP12, 7>(a, g, p, s, gbase, res);
+  } else {
+#pragma unroll
+    for (int sp = 0; sp < 4; sp++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) acc[sp][c] = mk<C>(0, 0);
+    do_hop<FT, S, COMP12, 0>(a, g, p, s, gbase, acc);
+    do_hop<FT, S, COMP12, 1>(a, g, p, s, gbase, acc);
+    do_hop<FT, S, COMP12, 2>(a, g, p, s, gbase, acc);
+    do_hop<FT, S, COMP12, 3>(a, g, p, s, gbase, acc);
+    do_hop<FT, S, COMP12, 4>(a, g, p, s, gbase, acc);
+    do_hop<FT, S, COMP12, 5>(a, g, p, s, gbase, acc);
+    do_hop<FT, S, COMP12, 6>(a, g, p, s, gbase, acc);
+    do_hop<FT, S, COMP12, 7>(a, g, p, s, gbase, acc);
+    if (FAM == FAM_CLOVER || FAM == FAM_TMCLOV) {
+      const long long cbase = tile * ((FAM == FAM_CLOVER ? 72LL : 144LL) * g.V) + lane;
+#pragma unroll
+      for (int blk = 0; blk < 2; blk++) {
+        if (FAM == FAM_CLOVER) clover_block<FT, false>(a.clov, cbase, g.V, blk, acc, res);
+        else full_clover_block<FT, false>(a.clov, cbase, g.V, blk, acc, res);
+      }
+    } else if (FAM == FAM_TM) {
+      inv_twisted<C, false>(acc, p.isPlus, p.mu, p.muinv, res);
+    } else {
+#pragma unroll
+      for (int sp = 0; sp < 4; sp++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) res[sp][c] = acc[sp][c];
+    }
+  }
+  store_spinor<FT, S>(a.out, obase, res);
+}
+
+} // namespace qb200

@@ -1,0 +1,109 @@
+"""ctypes binding of libqphix_b200.so (the C-ABI of include/qphix_b200.h).
+
+The library is built in-tree by qphix-codegen_b200/build.py.  There is no
+fallback: if the library is missing or a call fails, an exception is raised.
+"""
+import ctypes
+import os
+
+from .lattice import Lattice
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libqphix_b200.so")
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_U = ctypes.c_uint
+_D = ctypes.c_double
+_LAT = ctypes.POINTER(Lattice)
+_UA = ctypes.POINTER(ctypes.c_uint)
+_DA = ctypes.POINTER(ctypes.c_double)
+
+ERRORS = {-1: "QB200_EINVAL", -2: "QB200_ENULL", -3: "QB200_ELAYOUT", -4: "QB200_EDIR",
+          -5: "QB200_ECUDA", -6: "QB200_EALIGN", -7: "QB200_ENODEV"}
+
+# argument lists, in the order of include/qphix_b200.h
+_BODY = [_LAT, _I, _P, _P, _P, _UA, _D, _D, _D, _U, _DA, _P]
+_ACH = [_LAT, _I, _P, _P, _P, _P, _D, _D, _D, _D, _U, _DA, _UA, _P]
+_CLOV = [_LAT, _I, _P, _P, _P, _P, _UA, _D, _D, _D, _U, _DA, _P]
+_CLOV_ACH = [_LAT, _I, _P, _P, _P, _P, _P, _D, _D, _D, _U, _DA, _UA, _D, _P]
+_TM = [_LAT, _I, _P, _P, _P, _UA, _D, _D, _D, _U, _DA, _D, _D, _P]
+_TM_ACH = [_LAT, _I, _P, _P, _P, _P, _D, _D, _D, _D, _U, _DA, _D, _UA, _P]
+_PACK = [_LAT, _I, _P, _P, _I, _P]
+_FIN = [_LAT, _I, _P, _P, _P, _D, _I, _I, _DA, _P]
+_FIN_CLOV = [_LAT, _I, _P, _P, _P, _P, _D, _I, _I, _DA, _P]
+_FIN_TM = [_LAT, _I, _P, _P, _P, _D, _D, _D, _I, _I, _DA, _P]
+
+SIGNATURES = {}
+for _pm in ("plus", "minus"):
+    SIGNATURES.update({
+        "qb200_dslash_%s_vec" % _pm: _BODY,
+        "qb200_dslash_achimbdpsi_%s_vec" % _pm: _ACH,
+        "qb200_clov_dslash_%s_vec" % _pm: _CLOV,
+        "qb200_clov_dslash_achimbdpsi_%s_vec" % _pm: _CLOV_ACH,
+        "qb200_tm_dslash_%s_vec" % _pm: _TM,
+        "qb200_tm_dslash_achimbdpsi_%s_vec" % _pm: _TM_ACH,
+        "qb200_tm_clov_dslash_%s_vec" % _pm: _CLOV,
+        "qb200_tm_clov_dslash_achimbdpsi_%s_vec" % _pm: _CLOV_ACH,
+        "qb200_face_proj_dir_%s" % _pm: _PACK,
+        "qb200_face_finish_dir_%s" % _pm: _FIN,
+        "qb200_face_clov_finish_dir_%s" % _pm: _FIN_CLOV,
+        "qb200_tm_face_finish_dir_%s" % _pm: _FIN_TM,
+        "qb200_tm_clov_face_finish_dir_%s" % _pm: _FIN_CLOV,
+    })
+INFO = {
+    "qb200_abi_version": ([], _I),
+    "qb200_last_error": ([], ctypes.c_char_p),
+    "qb200_layout_supported": ([_I, _I], _I),
+    "qb200_spinor_elems": ([_LAT], ctypes.c_longlong),
+    "qb200_gauge_elems": ([_LAT], ctypes.c_longlong),
+    "qb200_clover_elems": ([_LAT], ctypes.c_longlong),
+    "qb200_full_clover_elems": ([_LAT], ctypes.c_longlong),
+    "qb200_face_sites": ([_LAT, _I], ctypes.c_longlong),
+}
+
+_lib = None
+
+
+class QB200Error(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (ERRORS.get(code, "error"), code, msg))
+        self.code = code
+
+
+def lib():
+    """Load libqphix_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libqphix_b200.so is not built: run python qphix-codegen_b200/build.py")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = _I
+        for name, (args, res) in INFO.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != 0:
+        raise QB200Error(rc, lib().qb200_last_error().decode())
+    return rc
+
+
+def uint8(vals):
+    if vals is None:
+        return None
+    arr = (ctypes.c_uint * 8)(*[int(v) for v in vals])
+    return arr
+
+
+def phases(ph):
+    if ph is None:
+        return None
+    flat = [float(v) for row in ph for v in row]
+    return (ctypes.c_double * 8)(*flat)

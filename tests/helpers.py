@@ -1,0 +1,70 @@
+"""Shared fixtures: seeded fields in the QPhiX layouts and comparison metrics."""
+import os
+import sys
+
+import numpy as np
+import torch
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(REPO, "qphix-codegen_b200")
+for p in (REPO, PKG):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+from qphix_b200 import fields, layout  # noqa: E402
+from qphix_b200.lattice import F16, F32, F64, Geometry  # noqa: E402
+
+NP_DTYPE = {F32: np.float32, F64: np.float64, F16: np.float16}
+FAMILIES = ("wilson", "clover", "tm", "tm_clover")
+KERNELS = ("dslash", "achimbdpsi")
+
+
+def make_fields(g: Geometry, seed=1234, cb=0, inverse_clover=False):
+    """Seeded inputs for checkerboard cb (out) / 1-cb (psi), as numpy arrays
+    in the storage type of g.  Keys: psi, chi, gauge, clover, fclover."""
+    U = fields.random_gauge(g, seed=seed)
+    psi = fields.random_spinor(g, seed=seed + 1)
+    chi = fields.random_spinor(g, seed=seed + 2)
+    A = fields.random_clover(g, seed=seed + 3)
+    if inverse_clover:
+        A = fields.invert_blocks(A)
+    F = fields.random_full_clover(g, seed=seed + 4)
+    dt = NP_DTYPE[g.ftype]
+    out = {
+        "U": U,
+        "psi": layout.pack_spinor(g, psi, torch.float64).numpy().astype(dt),
+        "chi": layout.pack_spinor(g, chi, torch.float64).numpy().astype(dt),
+        "gauge": layout.pack_gauge(g, U, cb, torch.float64).numpy().astype(dt),
+        "clover": layout.pack_clover(g, A, torch.float64).numpy().astype(dt),
+        "fclover": layout.pack_full_clover(g, F, torch.float64).numpy().astype(dt),
+    }
+    return out
+
+
+def site_rel_err(g: Geometry, a, b):
+    """max over components of |a-b| / max(|b_i|, |b_site|/sqrt(24)) -- the
+    per-component relative error with a floor at the site's rms component."""
+    a = np.asarray(a, dtype=np.float64)[: g.spinor_elems]
+    b = np.asarray(b, dtype=np.float64)[: g.spinor_elems]
+    ta = layout.unpack_spinor(g, torch.from_numpy(a)).numpy().reshape(-1, 12)
+    tb = layout.unpack_spinor(g, torch.from_numpy(b)).numpy().reshape(-1, 12)
+    ra = np.concatenate([ta.real, ta.imag], axis=1)
+    rb = np.concatenate([tb.real, tb.imag], axis=1)
+    site = np.sqrt((rb ** 2).sum(axis=1, keepdims=True) / 24.0)
+    den = np.maximum(np.abs(rb), site)
+    den = np.where(den == 0, 1.0, den)
+    return float((np.abs(ra - rb) / den).max())
+
+
+def op_params(family, kernel, seed=0, tbc_mask=0, accumulate=None, coeff=None):
+    """Scalar parameters used throughout the parity tests."""
+    rng = np.random.default_rng(seed)
+    ph = rng.normal(size=(4, 2))
+    ph = ph / np.linalg.norm(ph, axis=1, keepdims=True)
+    p = dict(coeff_s=0.91 if coeff is None else coeff, coeff_t_f=1.07, coeff_t_b=0.83,
+             alpha=1.3 if kernel == "achimbdpsi" else 1.0,
+             mu=0.21 if family == "tm" else 0.0,
+             muinv=0.77 if family == "tm" else 1.0,
+             rho=0.17 if family in ("clover", "tm_clover") and kernel == "achimbdpsi" else 0.0,
+             tbc_mask=tbc_mask, tbc_phases=ph.tolist(), accumulate=accumulate)
+    return p
