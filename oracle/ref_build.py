@@ -24,6 +24,7 @@ Usage: python oracle/ref_build.py [cfg ...]   (default: the DEFAULT list)
 """
 import concurrent.futures as cf
 import os
+import shutil
 import subprocess
 import sys
 
@@ -240,7 +241,9 @@ def build(name, jobs=8, opt="-O2"):
             futs.append(ex.submit(sh, ["g++"] + cflags + ["-c", s, "-o", o]))
         for fu in futs:
             fu.result()
-    sh(["g++", "-shared", "-fopenmp", "-o", so] + objs)
+    sh(["g++", "-shared", "-fopenmp", "-s", "-o", so] + objs)
+    # the generated sources and objects are large; only the library is kept
+    shutil.rmtree(cfgdir, ignore_errors=True)
     return so
 
 

@@ -7,8 +7,3 @@ seeded synthetic fields and thin torch wrappers of the C entry points.
 from .lattice import F16, F32, F64, Geometry, Lattice  # noqa: F401
 from . import fields, layout  # noqa: F401
 
-
-def ops():
-    """The torch wrappers (imports the CUDA library on first use)."""
-    from . import ops as _ops
-    return _ops

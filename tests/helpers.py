@@ -68,3 +68,16 @@ def op_params(family, kernel, seed=0, tbc_mask=0, accumulate=None, coeff=None):
              rho=0.17 if family in ("clover", "tm_clover") and kernel == "achimbdpsi" else 0.0,
              tbc_mask=tbc_mask, tbc_phases=ph.tolist(), accumulate=accumulate)
     return p
+
+
+def compress_gauge(g18: Geometry, gauge18):
+    """12-real gauge array (rows 0,1 of each stored link) from an 18-real one."""
+    a = np.asarray(gauge18).reshape(g18.ntiles, 8, 3, 3, 2, g18.veclen)
+    return np.ascontiguousarray(a[:, :, :2]).reshape(-1)
+
+
+def load_golden(ft):
+    """The golden vectors produced by tests/golden/make_golden.py."""
+    name = {F32: "scalar_f32", F64: "scalar_f64"}[ft]
+    path = os.path.join(REPO, "tests", "golden", "ref_%s_4x4x4x4.npz" % name)
+    return dict(np.load(path))

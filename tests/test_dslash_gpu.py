@@ -8,7 +8,6 @@ import torch
 
 import helpers as H
 import oracle as O
-from qphix_b200 import ops as _unused  # noqa: F401  (loads the ctypes wrappers lazily)
 from qphix_b200 import ops
 from qphix_b200.lattice import F16, F32, F64, Geometry
 
