@@ -1,0 +1,395 @@
+#!/usr/bin/env python3
+"""Benchmark of the headline configuration: Wilson-clover A.chi - b.D.psi
+(clov_dslash_achimbdpsi_plus) on a 32^3 x 64 lattice per GPU, FP32 storage
+and arithmetic, 12-real links, b = kappa = 0.125 (coeff_s = coeff_t = 0.125),
+rho = 0, clover blocks I + 0.1 H (H random Hermitian), random SU(3) links and
+Gaussian spinors (seeded, synthetic: the reference publishes no dataset).
+
+One step = one application of the operator to one checkerboard
+(V/2 = 1,048,576 sites on 32^3 x 64): 1824 flop/site (1320 Wilson + 504
+clover) and 960 algorithmic bytes/site (psi 96 + chi 96 + out 96 + 8 links
+x 48 + clover 288).  The fields (~1 GB) are larger than the 126 MB L2, so
+no flush is needed between steps.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+N > 1 (torchrun, one rank per GPU): weak scaling over t slabs, each rank
+holds a 32^3 x 64 slab of a 32^3 x 64N lattice; faces are exchanged with
+NCCL send/recv while the interior runs (qphix_b200.halo).
+--impl reference: the reference's own generated kernels (built from its
+sources into oracle/_ref) on all host cores, rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [REPO, os.path.join(REPO, "qphix-codegen_b200")]
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+FLOP_SITE = 1824
+METRIC = "Dslash GFLOP/s (clover A.chi - b.D.psi, 32^3x64 per GPU, FP32, 12-real links)"
+WORKLOAD = "clov_dslash_achimbdpsi_plus 32^3x64 FP32 compress12"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--soalen", type=int, default=16)
+    ap.add_argument("--veclen", type=int, default=0)
+    ap.add_argument("--dims", default="32,32,32,64")
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bound of the CPU baseline sample")
+    return ap.parse_args()
+
+
+def bytes_per_site(ft_bytes=4, rows=2):
+    return ft_bytes * (24 * 3 + 8 * rows * 6 + 72)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region (NVML, sampled every 20 ms)
+
+class ClockSampler:
+    REASONS = {
+        "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+        "sw_power_cap": 0x4, "hw_power_brake_slowdown": 0x80,
+    }
+
+    def __init__(self, index):
+        self.samples = []
+        self.reasons = 0
+        self.max_mhz = None
+        self._stop = threading.Event()
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+                self.reasons |= self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+            except Exception:
+                pass
+            time.sleep(0.02)
+
+    def __enter__(self):
+        if self.nv is not None:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self.nv is not None:
+            self._stop.set()
+            self.t.join()
+
+    def summary(self):
+        if self.nv is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"]}
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "samples": len(self.samples),
+                "reasons": [k for k, v in self.REASONS.items() if self.reasons & v]}
+
+
+def measured_peak():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_from_profile(workload_key):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (profiles/*.json), or None."""
+    p = os.path.join(REPO, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f).get(workload_key)
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+# fields
+
+def make_fields(g, device, cb=0, seed=1234):
+    from qphix_b200 import fields, layout
+    U = fields.random_gauge(g, seed=seed, device=device)
+    gauge = layout.pack_gauge(g, U, cb)
+    del U
+    psi = layout.pack_spinor(g, fields.random_spinor(g, seed=seed + 1, device=device))
+    chi = layout.pack_spinor(g, fields.random_spinor(g, seed=seed + 2, device=device))
+    clov = layout.pack_clover(g, fields.random_clover(g, seed=seed + 3, device=device))
+    return {"psi": psi, "chi": chi, "gauge": gauge, "clover": clov}
+
+
+PARAMS = dict(coeff_s=0.125, coeff_t_f=0.125, coeff_t_b=0.125, rho=0.0)
+
+
+# ---------------------------------------------------------------------------
+# CPU: the reference's generated kernels
+
+def pick_reference_lib():
+    import oracle as O
+    flags = open("/proc/cpuinfo").read()
+    for name, flag in (("avx512_f32_s16", "avx512f"), ("avx2_f32_s8", "avx2"), ("scalar_f32", "")):
+        if O.ref_available(name) and (not flag or flag in flags):
+            return name
+    return None
+
+
+def run_reference_cpu(dims, steps, warmup, seconds, fields_gpu=None, g_gpu=None):
+    """Time the reference kernels on the host; returns a dict."""
+    import oracle as O
+    from qphix_b200 import layout
+    from qphix_b200.lattice import Geometry
+    name = pick_reference_lib()
+    if name is None:
+        return {"unavailable": "reference kernels not built (python oracle/ref_build.py)"}
+    info = O.ref_info(name)
+    g = Geometry(*dims, soalen=info["soalen"], veclen=info["veclen"], compress12=True, t_boundary=-1.0)
+    if fields_gpu is not None:
+        # same canonical fields, repacked into the reference's layout
+        f = {}
+        for k, v in fields_gpu.items():
+            if k in ("psi", "chi"):
+                f[k] = layout.pack_spinor(g, layout.unpack_spinor(g_gpu, v)).cpu().numpy()
+            elif k == "gauge":
+                gg = layout.unpack_gauge(g_gpu, v)
+                r = torch.view_as_real(gg).reshape(g.nt, g.nz, g.ny, g.nxh, -1).to(torch.float32)
+                f[k] = layout._to_tiles(g, r).cpu().numpy()
+            else:
+                f[k] = layout.pack_clover(g, layout.unpack_clover(g_gpu, v)).cpu().numpy()
+    else:
+        f = {k: v.numpy() for k, v in make_fields(g, "cpu").items()}
+    A = {k: O.aligned(v) for k, v in f.items()}
+    out = O.aligned(np.zeros(g.spinor_elems, dtype=np.float32))
+    prm = O.make_params(**PARAMS)
+    nthreads = os.cpu_count() or 1
+    call = lambda: O.ref_dslash(name, g, "clover", "achimbdpsi", 1, 0, A["psi"], A["gauge"], chi=A["chi"],
+                                clover=A["clover"], params=prm, out=out, nthreads=nthreads)
+    for _ in range(max(1, warmup)):
+        call()
+    times = []
+    t_start = time.perf_counter()
+    for _ in range(max(1, steps)):
+        t0 = time.perf_counter()
+        call()
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start > seconds:
+            break
+    per = sum(times) / len(times)
+    gflops = FLOP_SITE * g.vol_cb / per / 1e9
+    return {"value": gflops, "unit": "GFLOP/s", "cores": nthreads, "kind": "reference",
+            "sample": "%d full-lattice calls of %s on %s (%s)" % (len(times), WORKLOAD, "x".join(map(str, dims)), name),
+            "ms_per_step": per * 1e3, "lib": name, "out": out}
+
+
+# ---------------------------------------------------------------------------
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "b200" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def reference_arm(args, world, rank):
+    dims = tuple(int(x) for x in args.dims.split(","))
+    if rank != 0:
+        return
+    r = run_reference_cpu(dims, args.steps, args.warmup, 1e9)
+    if "unavailable" in r:
+        print(json.dumps({"impl": "reference", "unavailable": r["unavailable"]}))
+        return
+    line = {
+        "metric": METRIC, "value": r["value"], "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+        "config": {"workload": WORKLOAD, "dims": list(dims), "layout": r["lib"], "host_threads": r["cores"]},
+        "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": r["value"], "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def b200_arm(args, world, rank, local):
+    import torch.distributed as dist
+    from qphix_b200 import ops
+    from qphix_b200.halo import GPUKernels, TComm, TSlabDslash
+    from qphix_b200.lattice import F32, Geometry
+
+    dev = torch.device("cuda", local)
+    dims = tuple(int(x) for x in args.dims.split(","))
+    G = Geometry(dims[0], dims[1], dims[2], dims[3] * world, soalen=args.soalen, veclen=args.veclen,
+                 ftype=F32, compress12=True, t_boundary=-1.0)
+    from qphix_b200.halo import local_geometry
+    g = local_geometry(G, rank, world)
+    f = make_fields(g, dev, seed=1234 + 17 * rank)
+    out = torch.zeros_like(f["psi"])
+    op = TSlabDslash(g, TComm(), GPUKernels(torch.float32, dev))
+    stream = torch.cuda.current_stream()
+
+    def step():
+        op.apply("clover", "achimbdpsi", 1, 0, f["psi"], out, f["gauge"], chi=f["chi"], clover=f["clover"],
+                 **PARAMS)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index if dev.index is not None else 0) as clk:
+        barrier()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        barrier()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    sites_all = g.vol_cb * world
+    gflops = FLOP_SITE * sites_all / (ms_step * 1e-3) / 1e9
+    launches_per_step = 1 if world == 1 else 5
+
+    # roofline of the body kernel: its own events over the same timed region
+    bps = bytes_per_site()
+    if world == 1:
+        launch_ms = ms_step
+    else:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        e0.record(stream)
+        for _ in range(args.steps):
+            ops.dslash(g, "clover", "achimbdpsi", 1, 0, f["psi"], out, f["gauge"], chi=f["chi"],
+                       clover=f["clover"], **PARAMS)
+        e1.record(stream)
+        barrier()
+        launch_ms = e0.elapsed_time(e1) / args.steps
+    achieved = bps * g.vol_cb / (launch_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peak()
+    key = "clov_dslash_achimbdpsi_f32_c12_s%d_v%d_%s" % (g.soalen, g.veclen, "x".join(map(str, dims)))
+    traffic = traffic_from_profile(key)
+
+    # e2e through the public API with host buffers: H2D psi, chi -> dslash -> D2H out
+    e2e = None
+    if world == 1 and args.e2e_steps > 0:
+        hpsi = f["psi"].cpu().pin_memory()
+        hchi = f["chi"].cpu().pin_memory()
+        hout = torch.empty_like(hpsi).pin_memory()
+        dpsi, dchi = torch.empty_like(f["psi"]), torch.empty_like(f["chi"])
+
+        def e2e_step():
+            dpsi.copy_(hpsi, non_blocking=True)
+            dchi.copy_(hchi, non_blocking=True)
+            ops.dslash(g, "clover", "achimbdpsi", 1, 0, dpsi, out, f["gauge"], chi=dchi, clover=f["clover"],
+                       **PARAMS)
+            hout.copy_(out, non_blocking=True)
+
+        for _ in range(2):
+            e2e_step()
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        a1.record(stream)
+        torch.cuda.synchronize()
+        e_ms = a0.elapsed_time(a1) / args.e2e_steps
+        nb = f["psi"].numel() * 4
+        e2e = {"value": FLOP_SITE * g.vol_cb / (e_ms * 1e-3) / 1e9, "unit": "GFLOP/s",
+               "h2d_bytes_per_step": 2 * nb, "d2h_bytes_per_step": nb, "ms_per_step": e_ms,
+               "path": "qb200_clov_dslash_achimbdpsi_plus_vec via ctypes, pinned host buffers"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = run_reference_cpu(dims, 1000, 1, args.cpu_seconds, fields_gpu=f, g_gpu=g)
+        if "unavailable" in r:
+            cpu = {"unavailable": r["unavailable"]}
+        else:
+            cpu = {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            # same inputs: the reference result must match the GPU one
+            from qphix_b200 import layout
+            import oracle as O
+            info = O.ref_info(r["lib"])
+            gr = g.with_(soalen=info["soalen"], veclen=info["veclen"])
+            ops.dslash(g, "clover", "achimbdpsi", 1, 0, f["psi"], out, f["gauge"], chi=f["chi"],
+                       clover=f["clover"], **PARAMS)
+            a = layout.unpack_spinor(g, out.cpu())
+            b = layout.unpack_spinor(gr, torch.from_numpy(r["out"][: gr.spinor_elems].copy()))
+            cpu["max_abs_diff_vs_gpu"] = float((a - b).abs().max())
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": gflops, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "dims_per_gpu": list(dims), "global_dims": list(G.dims),
+                       "soalen": g.soalen, "veclen": g.veclen, "cb_sites_per_gpu": g.vol_cb,
+                       "parallelism": "t-slab halo over %d GPUs" % world if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (%.2f GB per step)" % (bps * g.vol_cb / 1e9),
+                       "flop_per_site": FLOP_SITE, "bytes_per_site": bps},
+            "gbs": achieved,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel_ms": launch_ms},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            reference_arm(args, world, rank)
+        else:
+            b200_arm(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

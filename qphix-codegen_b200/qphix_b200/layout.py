@@ -67,11 +67,14 @@ def unpack_spinor(g: Geometry, flat: torch.Tensor) -> torch.Tensor:
     return torch.view_as_complex(b)
 
 
-def site_links(g: Geometry, U: torch.Tensor, cb: int) -> torch.Tensor:
+def site_links(g: Geometry, U: torch.Tensor, cb: int, t0: int = 0) -> torch.Tensor:
     """The eight links each site of cb uses, as U (not transposed):
-    (nt, nz, ny, nxh, 8, 3, 3)."""
+    (nt, nz, ny, nxh, 8, 3, 3).  U may cover a longer time extent than g
+    (a global lattice of which g is the slab starting at time slice t0)."""
     x, y, z, t = cb_coords(g, cb, U.device)
-    L = [g.nx, g.ny, g.nz, g.nt]
+    NT = U.shape[1]
+    t = (t + t0) % NT
+    L = [g.nx, g.ny, g.nz, NT]
     links = []
     for mu in range(4):
         c = [x, y, z, t]
@@ -97,10 +100,11 @@ def _from_tiles(g: Geometry, flat: torch.Tensor, K: int) -> torch.Tensor:
     return v.reshape(g.nt, g.nz, g.ny, g.nxh, K)
 
 
-def pack_gauge(g: Geometry, U: torch.Tensor, cb: int, dtype=None) -> torch.Tensor:
-    """Full-lattice links -> SU3MatrixBlock array of checkerboard cb."""
+def pack_gauge(g: Geometry, U: torch.Tensor, cb: int, dtype=None, t0: int = 0) -> torch.Tensor:
+    """Full-lattice links -> SU3MatrixBlock array of checkerboard cb (of the
+    slab of g that starts at global time slice t0)."""
     dtype = dtype or g.dtype
-    G = site_links(g, U.to(torch.complex128), cb).transpose(-1, -2)   # G = U^T
+    G = site_links(g, U.to(torch.complex128), cb, t0).transpose(-1, -2)   # G = U^T
     G = G[..., : g.rows, :]
     r = torch.view_as_real(G).reshape(g.nt, g.nz, g.ny, g.nxh, 8 * g.rows * 6)
     return _to_tiles(g, r).to(dtype).contiguous()
