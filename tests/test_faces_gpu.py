@@ -1,0 +1,115 @@
+"""GPU face kernels against the oracle, and the t-slab decomposition (body
+without slab-crossing hops + face pack/exchange/unpack) emulated on one GPU
+against the full-lattice kernel."""
+import numpy as np
+import pytest
+import torch
+
+import helpers as H
+import oracle as O
+from qphix_b200 import fields, layout, ops
+from qphix_b200.halo import GPUKernels, face_kind, local_geometry
+from qphix_b200.lattice import F16, F32, F64, Geometry
+
+pytestmark = pytest.mark.gpu
+TOL = {F32: 2e-6, F64: 1e-13, F16: 1e-3}
+LAYOUTS = [(1, 1, F32), (4, 16, F32), (16, 16, F32), (2, 4, F64), (8, 8, F16)]
+
+
+@pytest.mark.parametrize("soa,vec,ft", LAYOUTS)
+def test_face_pack(cuda, soa, vec, ft):
+    g = Geometry(max(4, 2 * soa), 8, 4, 6, soalen=soa, veclen=vec, ftype=ft)
+    f = H.make_fields(g, cb=0, seed=31)
+    psi = torch.from_numpy(f["psi"]).to(cuda)
+    for d in range(8):
+        for isign in (1, -1):
+            buf = torch.zeros(12 * g.face_sites(d), dtype=g.dtype, device=cuda)
+            ops.face_pack(g, isign, 1, psi, buf, d)
+            ref = O.face_pack(g, isign, 1, f["psi"], d)
+            a = buf.cpu().numpy().astype(np.float64)
+            scale = np.abs(ref).max()
+            assert np.abs(a - ref).max() <= TOL[ft] * scale * 4, (d, isign)
+
+
+@pytest.mark.parametrize("soa,vec,ft", LAYOUTS)
+def test_face_unpack(cuda, soa, vec, ft):
+    g = Geometry(max(4, 2 * soa), 8, 4, 6, soalen=soa, veclen=vec, ftype=ft, compress12=(soa % 2 == 0))
+    f = H.make_fields(g, cb=0, seed=32)
+    rng = np.random.default_rng(5)
+    for fam in H.FAMILIES:
+        cl_np = f["fclover" if fam == "tm_clover" else "clover"]
+        cl = torch.from_numpy(cl_np).to(cuda)
+        gauge = torch.from_numpy(f["gauge"]).to(cuda)
+        for d in range(8):
+            for isign in (1, -1):
+                n = g.face_sites(d)
+                inbuf_np = rng.normal(size=12 * n).astype(f["psi"].dtype)
+                pp = H.op_params(fam, "dslash")
+                tbc = (d + isign) % 3 == 0
+                out = torch.from_numpy(f["chi"]).to(cuda)
+                ops.face_unpack(g, fam, isign, 0, torch.from_numpy(inbuf_np).to(cuda), gauge, out, d, beta=0.41,
+                                clover=cl, mu=pp["mu"], muinv=pp["muinv"], tbc=tbc, tbc_phases=pp["tbc_phases"])
+                ref = O.face_unpack(g, fam, isign, 0, inbuf_np, f["gauge"], f["chi"].copy(), d, beta=0.41,
+                                    clover=cl_np, mu=pp["mu"], muinv=pp["muinv"], tbc=tbc,
+                                    tbc_phases=pp["tbc_phases"])
+                e = H.site_rel_err(g, out.cpu().numpy(), ref)
+                assert e < TOL[ft], (fam, d, isign, e)
+
+
+@pytest.mark.parametrize("ft", [F32, F64])
+def test_two_slab_decomposition_on_one_gpu(cuda, ft):
+    """Two t slabs driven on one device: pack both, swap the face buffers,
+    then interior + unpack per slab; must equal the undecomposed operator."""
+    G = Geometry(8, 8, 4, 8, soalen=4, veclen=8, ftype=ft, compress12=True, t_boundary=-1.0)
+    cb = 0
+    U = fields.random_gauge(G, seed=41)
+    psi, chi = fields.random_spinor(G, seed=42), fields.random_spinor(G, seed=43)
+    A, F = fields.random_clover(G, seed=44), fields.random_full_clover(G, seed=45)
+    D = lambda t: t.to(cuda)
+    full = {"psi": D(layout.pack_spinor(G, psi)), "chi": D(layout.pack_spinor(G, chi)),
+            "gauge": D(layout.pack_gauge(G, U, cb)), "clover": D(layout.pack_clover(G, A)),
+            "fclover": D(layout.pack_full_clover(G, F))}
+    slabs = []
+    for r in range(2):
+        g = local_geometry(G, r, 2)
+        sl = slice(r * g.nt, (r + 1) * g.nt)
+        slabs.append((g, {"psi": D(layout.pack_spinor(g, psi[sl])), "chi": D(layout.pack_spinor(g, chi[sl])),
+                          "gauge": D(layout.pack_gauge(g, U, cb, t0=r * g.nt)),
+                          "clover": D(layout.pack_clover(g, A[sl])), "fclover": D(layout.pack_full_clover(g, F[sl]))}))
+    K = GPUKernels(G.dtype, cuda)
+    for fam in H.FAMILIES:
+        for kernel in H.KERNELS:
+            for isign in (1, -1):
+                pp = H.op_params(fam, kernel, tbc_mask=8)
+                pp.pop("accumulate")
+                clk = "fclover" if fam == "tm_clover" else "clover"
+                ref = torch.zeros_like(full["psi"])
+                ops.dslash(G, fam, kernel, isign, cb, full["psi"], ref, full["gauge"], chi=full["chi"],
+                           clover=full[clk], **pp)
+                ref_c = layout.unpack_spinor(G, ref.cpu())
+                # face buffers: [rank] -> (to forward, to backward)
+                sends = []
+                for g, f in slabs:
+                    n = g.face_sites(6)
+                    bf, bb = K.alloc(12 * n), K.alloc(12 * n)
+                    K.pack(g, isign, 1 - cb, f["psi"], bf, 7)
+                    K.pack(g, isign, 1 - cb, f["psi"], bb, 6)
+                    sends.append((bf, bb))
+                kind, sg = face_kind(fam, kernel)
+                for r, (g, f) in enumerate(slabs):
+                    out = torch.zeros_like(f["psi"])
+                    K.body(g, fam, kernel, isign, cb, f["psi"], out, f["gauge"], accumulate=[1] * 6 + [0, 0],
+                           chi=f["chi"], clover=f[clk], **pp)
+                    from_back = sends[(r - 1) % 2][0]
+                    from_fwd = sends[(r + 1) % 2][1]
+                    bb = sg * pp["coeff_t_b"] * (G.t_boundary if g.t_edge_lo else 1.0)
+                    bfw = sg * pp["coeff_t_f"] * (G.t_boundary if g.t_edge_hi else 1.0)
+                    cl = f[clk] if kind in ("clover", "tm_clover") else None
+                    K.unpack(g, kind, isign, cb, from_back, f["gauge"], out, 6, beta=bb, clover=cl, mu=pp["mu"],
+                             muinv=pp["muinv"], tbc=True, tbc_phases=pp["tbc_phases"])
+                    K.unpack(g, kind, isign, cb, from_fwd, f["gauge"], out, 7, beta=bfw, clover=cl, mu=pp["mu"],
+                             muinv=pp["muinv"], tbc=True, tbc_phases=pp["tbc_phases"])
+                    got = layout.unpack_spinor(g, out.cpu())
+                    exp = ref_c[r * g.nt:(r + 1) * g.nt]
+                    err = float((got - exp).abs().max() / exp.abs().max())
+                    assert err < (2e-6 if ft == F32 else 1e-13), (fam, kernel, isign, r, err)
