@@ -6,7 +6,7 @@
 #include <cstring>
 #include <string>
 
-#include "../../include/qphix_b200.h"
+#include "qphix_b200.h"
 #include "qb200_internal.h"
 
 using namespace qb200;
