@@ -316,6 +316,72 @@ int qb200_tm_clov_face_finish_dir_minus(const qb200_lattice *lat, int cb,
                                         const double *tbc_phases,
                                         void *stream);
 
+/*
+ * ---- even-odd operator, BLAS and solvers ---------------------------------
+ * Not part of the reference (its caller, QPhiX, builds these from the
+ * kernels); provided so that a GPU caller needs no per-iteration host code.
+ *
+ * The Schur operator on checkerboard o = target_cb (e = 1 - o):
+ *   Mhat psi = A_oo psi - D_oe A_ee^-1 D_eo psi   (hops scaled by coeff_*)
+ * built as the plain kernel on e (with the inverse diagonal term) followed by
+ * the achimbdpsi kernel on o.  Per family:
+ *   wilson     A = alpha (the plain hop is scaled by 1/alpha)
+ *   clover     clov[o] = A_oo (CloverBlock), clov[e] = A_ee^-1
+ *   tm         A = alpha (1 + i mu g5); mu, muinv as in tm_dslash
+ *   tm_clover  clov[o] = F_oo, clov[e] = F_ee^-1 (FullCloverBlock);
+ *              clov_dag[] = the same blocks conjugate-transposed (dagger)
+ * isign = -1 applies Mhat^dag (the minus kernels, D^dag = D(isign=-1)).
+ */
+typedef struct qb200_operator {
+  int family; /* 0 wilson, 1 clover, 2 tm, 3 tm_clover */
+  int target_cb;
+  const void *gauge[2];     /* packed links of checkerboard 0 and 1 */
+  const void *clov[2];      /* see above, indexed by checkerboard */
+  const void *clov_dag[2];  /* tm_clover only */
+  double coeff_s, coeff_t_f, coeff_t_b;
+  double alpha, mu, muinv, rho;
+  unsigned tbc_mask;
+  double tbc_phases[4][2];
+} qb200_operator;
+
+/* out = Mhat in (isign +1) or Mhat^dag in (-1); tmp_other_cb: one spinor */
+int qb200_schur_apply(const qb200_lattice *lat, const qb200_operator *op, int isign, const void *in, void *out,
+                      void *tmp_other_cb, void *stream);
+
+/* BLAS on n storage elements (a whole spinor array, padding included).
+ * Reductions accumulate in FP64 and leave the result on the device;
+ * `partials` is device scratch of qb200_blas_partials_len() doubles. */
+long long qb200_blas_partials_len(void);
+int qb200_blas_axpby(int ftype, long long n, double a, const void *x, double b, void *y, void *stream);
+int qb200_blas_convert(int ft_out, void *out, int ft_in, const void *in, long long n, double scale,
+                       void *stream);
+int qb200_blas_dot(int ftype, long long n, const void *x, const void *y, double *result, double *partials,
+                   void *stream);
+int qb200_blas_cdot(const qb200_lattice *lat, const void *x, const void *y, double *result /* re, im */,
+                    double *partials, void *stream);
+
+/* Solvers for Mhat x = b on the target checkerboard.  Device workspace of
+ * the size the *_workspace_bytes function returns is passed by the caller.
+ * rel_res returns |b - Mhat x| / |b|.  CG runs on the normal equations. */
+long long qb200_cg_workspace_bytes(const qb200_lattice *lat);
+long long qb200_bicgstab_workspace_bytes(const qb200_lattice *lat);
+int qb200_invert_cg(const qb200_lattice *lat, const qb200_operator *op, const void *b, void *x, double rel_tol,
+                    int max_iter, void *workspace, int *iters, double *rel_res, void *stream);
+int qb200_invert_bicgstab(const qb200_lattice *lat, const qb200_operator *op, const void *b, void *x,
+                          double rel_tol, int max_iter, void *workspace, int *iters, double *rel_res,
+                          void *stream);
+/* Mixed precision with defect correction: residuals and the solution in the
+ * high-precision lattice (FP64 storage), corrections solved with the
+ * low-precision lattice (FP32 or FP16 storage; its operator fields in that
+ * type) to inner_tol.  solver 0: CG on the normal equations, 1: BiCGStab.
+ * Returns the high workspace size; *lo_bytes receives the low one. */
+long long qb200_mixed_workspace_bytes(const qb200_lattice *lat_hi, const qb200_lattice *lat_lo,
+                                      long long *lo_bytes);
+int qb200_invert_mixed(const qb200_lattice *lat_hi, const qb200_operator *op_hi, const qb200_lattice *lat_lo,
+                       const qb200_operator *op_lo, int solver, const void *b, void *x, double rel_tol,
+                       double inner_tol, int max_inner, int max_outer, void *ws_hi, void *ws_lo,
+                       int *inner_iters, int *outer_iters, double *rel_res, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -36,7 +36,8 @@ def nvcc():
 
 def units():
     """(object path, extra flags, source) for every translation unit."""
-    out = [(os.path.join(BUILD, "qb200_api.o"), [], os.path.join(CSRC, "qb200_api.cu"))]
+    out = [(os.path.join(BUILD, "qb200_api.o"), [], os.path.join(CSRC, "qb200_api.cu")),
+           (os.path.join(BUILD, "qb200_solver.o"), [], os.path.join(CSRC, "qb200_solver.cu"))]
     for tag, ft in FTYPES.items():
         for s in SOALENS:
             out.append((os.path.join(BUILD, "inst_%s_s%d.o" % (tag, s)),

@@ -300,6 +300,40 @@ long long elem_count(const qb200_lattice *l, int what)
 
 } // namespace
 
+namespace qb200 {
+// shared with the solver translation unit
+int api_fail(int code, const char *msg) { return fail(code, "%s", msg); }
+
+int api_body(const qb200_lattice *l, int fam, bool ach, int isPlus, int cb, const void *psi, const void *chi,
+             const void *gauge, const void *clov, void *out, const unsigned *accumulate, double coeff_s,
+             double coeff_t_f, double coeff_t_b, unsigned tbc_mask, const double *tbc_phases, double alpha,
+             double mu, double muinv, double rho, void *stream)
+{
+  Body b;
+  std::memset(&b, 0, sizeof(b));
+  b.fam = fam;
+  b.ach = ach;
+  b.isPlus = isPlus;
+  b.cb = cb;
+  b.psi = psi;
+  b.chi = chi;
+  b.gauge = gauge;
+  b.clov = clov;
+  b.out = out;
+  b.accumulate = accumulate;
+  b.coeff_s = coeff_s;
+  b.coeff_t_f = coeff_t_f;
+  b.coeff_t_b = coeff_t_b;
+  b.tbc_mask = tbc_mask;
+  b.tbc_phases = tbc_phases;
+  b.alpha = alpha;
+  b.mu = mu;
+  b.muinv = muinv;
+  b.rho = rho;
+  return run_body(l, b, stream);
+}
+} // namespace qb200
+
 extern "C" {
 
 int qb200_abi_version(void) { return QB200_ABI_VERSION; }

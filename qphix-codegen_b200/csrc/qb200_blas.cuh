@@ -1,0 +1,195 @@
+// qb200_blas.cuh -- level-1 linear algebra on spinor fields for the solvers.
+//
+// Fields are whole QPhiX spinor arrays (padding included; padding stays zero
+// because every operation is linear and the inputs' padding is zero).
+// Element-wise operations stream 16-byte vectors; reductions accumulate in
+// FP64 per thread, reduce per block, and write one partial per block into a
+// scratch array that a one-block finishing kernel sums into a double on the
+// device (results stay on the device so that a solver iteration needs no
+// host synchronisation).
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+namespace qb200 {
+
+// grid of the reduction kernels: 4 blocks of 256 threads per SM of a B200
+constexpr int kRedThreads = 256;
+constexpr int kRedBlocks = 148 * 4;
+// doubles of scratch one reduction needs (two components for complex dots)
+constexpr int kRedPartials = 2 * kRedBlocks;
+
+// number of storage elements moved per 16-byte vector
+template <typename FT> struct vec16;
+template <> struct vec16<float> {
+  static constexpr int n = 4;
+};
+template <> struct vec16<double> {
+  static constexpr int n = 2;
+};
+template <> struct vec16<__half> {
+  static constexpr int n = 8;
+};
+
+template <typename FT> __device__ __forceinline__ double to_d(FT v);
+template <> __device__ __forceinline__ double to_d<float>(float v) { return (double)v; }
+template <> __device__ __forceinline__ double to_d<double>(double v) { return v; }
+template <> __device__ __forceinline__ double to_d<__half>(__half v) { return (double)__half2float(v); }
+
+template <typename FT> __device__ __forceinline__ FT from_d(double v);
+template <> __device__ __forceinline__ float from_d<float>(double v) { return (float)v; }
+template <> __device__ __forceinline__ double from_d<double>(double v) { return v; }
+template <> __device__ __forceinline__ __half from_d<__half>(double v) { return __float2half_rn((float)v); }
+
+template <typename FT> struct V16 {
+  FT e[vec16<FT>::n];
+};
+
+template <typename FT> __device__ __forceinline__ V16<FT> ld16(const FT *p)
+{
+  V16<FT> v;
+  *reinterpret_cast<uint4 *>(&v) = __ldg(reinterpret_cast<const uint4 *>(p));
+  return v;
+}
+
+template <typename FT> __device__ __forceinline__ void st16(FT *p, const V16<FT> &v)
+{
+  *reinterpret_cast<uint4 *>(p) = *reinterpret_cast<const uint4 *>(&v);
+}
+
+// ---------------------------------------------------------------------------
+// element-wise: y = a*x + b*y, with a and b from the host or from device
+// scalars (a_dev/b_dev non-null: a = a_scale * a_dev[0] (or its ratio form))
+
+struct ScalarRef {
+  double host;          // used when dev == nullptr
+  const double *num;    // device numerator
+  const double *den;    // device denominator (nullptr: 1)
+  double sign;
+  __device__ __forceinline__ double get() const
+  {
+    if (!num) return host;
+    return sign * (den ? num[0] / den[0] : num[0]);
+  }
+};
+
+template <typename FT>
+__global__ void __launch_bounds__(256) axpby_kernel(long long nv, ScalarRef a, const FT *__restrict__ x,
+                                                    ScalarRef b, FT *__restrict__ y)
+{
+  const double av = a.get(), bv = b.get();
+  constexpr int W = vec16<FT>::n;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv;
+       i += (long long)gridDim.x * blockDim.x) {
+    V16<FT> vx = ld16(x + i * W);
+    V16<FT> vy = ld16(y + i * W);
+#pragma unroll
+    for (int k = 0; k < W; k++) vy.e[k] = from_d<FT>(av * to_d(vx.e[k]) + bv * to_d(vy.e[k]));
+    st16(y + i * W, vy);
+  }
+}
+
+// out = scale * in with conversion of the storage type
+template <typename FO, typename FI>
+__global__ void __launch_bounds__(256) convert_kernel(long long n, double scale, const FI *__restrict__ in,
+                                                      FO *__restrict__ out)
+{
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = from_d<FO>(scale * to_d(in[i]));
+}
+
+// ---------------------------------------------------------------------------
+// reductions
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// block sum of two values; thread 0 holds the result
+__device__ __forceinline__ void block_sum2(double &a, double &b)
+{
+  __shared__ double sa[32], sb[32];
+  a = warp_sum(a);
+  b = warp_sum(b);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    sa[w] = a;
+    sb[w] = b;
+  }
+  __syncthreads();
+  if (w == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    a = l < nw ? sa[l] : 0.0;
+    b = l < nw ? sb[l] : 0.0;
+    a = warp_sum(a);
+    b = warp_sum(b);
+  }
+}
+
+// partials[blockIdx.x] = sum x*y (real dot; x == y gives the norm squared)
+template <typename FT>
+__global__ void __launch_bounds__(kRedThreads) dot_partial_kernel(long long nv, const FT *__restrict__ x,
+                                                                  const FT *__restrict__ y,
+                                                                  double *__restrict__ partials)
+{
+  constexpr int W = vec16<FT>::n;
+  double s = 0.0, dummy = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv;
+       i += (long long)gridDim.x * blockDim.x) {
+    V16<FT> vx = ld16(x + i * W);
+    V16<FT> vy = ld16(y + i * W);
+#pragma unroll
+    for (int k = 0; k < W; k++) s += to_d(vx.e[k]) * to_d(vy.e[k]);
+  }
+  block_sum2(s, dummy);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+// complex dot <x, y> = sum conj(x) y over a QPhiX spinor field: the real and
+// imaginary parts of a component are S elements apart within a block
+template <typename FT, int S>
+__global__ void __launch_bounds__(kRedThreads) cdot_partial_kernel(long long npairs, const FT *__restrict__ x,
+                                                                   const FT *__restrict__ y,
+                                                                   double *__restrict__ partials)
+{
+  double re = 0.0, im = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < npairs;
+       i += (long long)gridDim.x * blockDim.x) {
+    // pair i: group g = i / S of 2S elements, lane i % S
+    const long long g = i / S;
+    const int l = (int)(i - g * S);
+    const long long e = g * 2 * S + l;
+    const double xr = to_d(x[e]), xi = to_d(x[e + S]);
+    const double yr = to_d(y[e]), yi = to_d(y[e + S]);
+    re += xr * yr + xi * yi;
+    im += xr * yi - xi * yr;
+  }
+  block_sum2(re, im);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = re;
+    partials[kRedBlocks + blockIdx.x] = im;
+  }
+}
+
+// result[c] = sum of partials[c*kRedBlocks .. +nblocks) for c < ncomp
+__global__ void __launch_bounds__(kRedThreads) finish_kernel(const double *__restrict__ partials, int nblocks,
+                                                             int ncomp, double *__restrict__ result)
+{
+  double a = 0.0, b = 0.0;
+  for (int i = threadIdx.x; i < nblocks; i += blockDim.x) {
+    a += partials[i];
+    if (ncomp > 1) b += partials[kRedBlocks + i];
+  }
+  block_sum2(a, b);
+  if (threadIdx.x == 0) {
+    result[0] = a;
+    if (ncomp > 1) result[1] = b;
+  }
+}
+
+} // namespace qb200

@@ -61,6 +61,40 @@ INFO = {
     "qb200_face_sites": ([_LAT, _I], ctypes.c_longlong),
 }
 
+
+
+class Operator(ctypes.Structure):
+    """ctypes mirror of `qb200_operator`."""
+    _fields_ = [
+        ("family", ctypes.c_int), ("target_cb", ctypes.c_int),
+        ("gauge", ctypes.c_void_p * 2), ("clov", ctypes.c_void_p * 2), ("clov_dag", ctypes.c_void_p * 2),
+        ("coeff_s", ctypes.c_double), ("coeff_t_f", ctypes.c_double), ("coeff_t_b", ctypes.c_double),
+        ("alpha", ctypes.c_double), ("mu", ctypes.c_double), ("muinv", ctypes.c_double), ("rho", ctypes.c_double),
+        ("tbc_mask", ctypes.c_uint), ("tbc_phases", (ctypes.c_double * 2) * 4),
+    ]
+
+
+_OP = ctypes.POINTER(Operator)
+_DP = ctypes.POINTER(ctypes.c_double)
+_IP = ctypes.POINTER(ctypes.c_int)
+_LL = ctypes.c_longlong
+SIGNATURES.update({
+    "qb200_schur_apply": [_LAT, _OP, _I, _P, _P, _P, _P],
+    "qb200_blas_axpby": [_I, _LL, _D, _P, _D, _P, _P],
+    "qb200_blas_convert": [_I, _P, _I, _P, _LL, _D, _P],
+    "qb200_blas_dot": [_I, _LL, _P, _P, _P, _P, _P],
+    "qb200_blas_cdot": [_LAT, _P, _P, _P, _P, _P],
+    "qb200_invert_cg": [_LAT, _OP, _P, _P, _D, _I, _P, _IP, _DP, _P],
+    "qb200_invert_bicgstab": [_LAT, _OP, _P, _P, _D, _I, _P, _IP, _DP, _P],
+    "qb200_invert_mixed": [_LAT, _OP, _LAT, _OP, _I, _P, _P, _D, _D, _I, _I, _P, _P, _IP, _IP, _DP, _P],
+})
+INFO.update({
+    "qb200_blas_partials_len": ([], _LL),
+    "qb200_cg_workspace_bytes": ([_LAT], _LL),
+    "qb200_bicgstab_workspace_bytes": ([_LAT], _LL),
+    "qb200_mixed_workspace_bytes": ([_LAT, _LAT, ctypes.POINTER(_LL)], _LL),
+})
+
 _lib = None
 
 

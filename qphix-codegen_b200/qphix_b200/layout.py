@@ -52,7 +52,7 @@ def pack_spinor(g: Geometry, sp: torch.Tensor, dtype=None) -> torch.Tensor:
     """Canonical checkerboard spinor -> FourSpinorBlock array (flat)."""
     dtype = dtype or g.dtype
     S = g.soalen
-    r = torch.view_as_real(sp.to(torch.complex128))          # nt nz ny nxh 4 3 2
+    r = torch.view_as_real(sp.to(torch.complex128).resolve_conj())        # nt nz ny nxh 4 3 2
     r = r.reshape(g.nt, g.nz, g.ny, g.nvecs, S, 4, 3, 2)
     r = r.permute(0, 1, 2, 3, 6, 5, 7, 4)                    # .. nvecs c s ri S
     return _blocks_to_flat(g, r.reshape(g.nt, g.nz, g.ny, g.nvecs, 24 * S).to(dtype))
@@ -106,7 +106,7 @@ def pack_gauge(g: Geometry, U: torch.Tensor, cb: int, dtype=None, t0: int = 0) -
     dtype = dtype or g.dtype
     G = site_links(g, U.to(torch.complex128), cb, t0).transpose(-1, -2)   # G = U^T
     G = G[..., : g.rows, :]
-    r = torch.view_as_real(G).reshape(g.nt, g.nz, g.ny, g.nxh, 8 * g.rows * 6)
+    r = torch.view_as_real(G.resolve_conj()).reshape(g.nt, g.nz, g.ny, g.nxh, 8 * g.rows * 6)
     return _to_tiles(g, r).to(dtype).contiguous()
 
 
@@ -134,7 +134,7 @@ def pack_clover(g: Geometry, A: torch.Tensor, dtype=None) -> torch.Tensor:
     rows, cols = _tril_index()
     diag = torch.diagonal(A, dim1=-2, dim2=-1).real              # ... 2 6
     off = A[..., rows, cols]                                      # ... 2 15
-    off = torch.view_as_real(off).reshape(*off.shape[:-1], 30)    # ... 2 30
+    off = torch.view_as_real(off.resolve_conj()).reshape(*off.shape[:-1], 30)    # ... 2 30
     per = torch.cat([diag, off], dim=-1).reshape(g.nt, g.nz, g.ny, g.nxh, 72)
     return _to_tiles(g, per).to(dtype).contiguous()
 
@@ -154,7 +154,7 @@ def unpack_clover(g: Geometry, flat: torch.Tensor) -> torch.Tensor:
 def pack_full_clover(g: Geometry, F: torch.Tensor, dtype=None) -> torch.Tensor:
     """Dense complex blocks (nt,nz,ny,nxh,2,6,6) -> FullCloverBlock array."""
     dtype = dtype or g.dtype
-    r = torch.view_as_real(F.to(torch.complex128)).reshape(g.nt, g.nz, g.ny, g.nxh, 144)
+    r = torch.view_as_real(F.to(torch.complex128).resolve_conj()).reshape(g.nt, g.nz, g.ny, g.nxh, 144)
     return _to_tiles(g, r).to(dtype).contiguous()
 
 

@@ -81,3 +81,55 @@ def load_golden(ft):
     name = {F32: "scalar_f32", F64: "scalar_f64"}[ft]
     path = os.path.join(REPO, "tests", "golden", "ref_%s_4x4x4x4.npz" % name)
     return dict(np.load(path))
+
+
+def eo_setup(g: Geometry, family, seed=900, target_cb=1, kappa=0.12):
+    """Fields and parameters of the even-odd operator of `family` on both
+    checkerboards (numpy, storage type of g).  Returns (fields, params):
+    fields: gauge[cb], clov[cb] (A on target_cb, A^-1 on the other; dense
+    F / F^-1 for tm_clover), clov_dag[cb] (tm_clover), b (source on target_cb)."""
+    dt = NP_DTYPE[g.ftype]
+    U = fields.random_gauge(g, seed=seed)
+    other = 1 - target_cb
+    f = {"gauge": [None, None], "clov": [None, None], "clov_dag": [None, None]}
+    for cb in (0, 1):
+        f["gauge"][cb] = layout.pack_gauge(g, U, cb, torch.float64).numpy().astype(dt)
+    if family == "clover":
+        A_t = fields.random_clover(g, seed=seed + 1)
+        A_o = fields.random_clover(g, seed=seed + 2)
+        f["clov"][target_cb] = layout.pack_clover(g, A_t, torch.float64).numpy().astype(dt)
+        f["clov"][other] = layout.pack_clover(g, fields.invert_blocks(A_o), torch.float64).numpy().astype(dt)
+    if family == "tm_clover":
+        F_t = fields.random_full_clover(g, seed=seed + 1)
+        F_o = fields.invert_blocks(fields.random_full_clover(g, seed=seed + 2))
+        f["clov"][target_cb] = layout.pack_full_clover(g, F_t, torch.float64).numpy().astype(dt)
+        f["clov"][other] = layout.pack_full_clover(g, F_o, torch.float64).numpy().astype(dt)
+        f["clov_dag"][target_cb] = layout.pack_full_clover(g, F_t.conj().transpose(-1, -2),
+                                                           torch.float64).numpy().astype(dt)
+        f["clov_dag"][other] = layout.pack_full_clover(g, F_o.conj().transpose(-1, -2),
+                                                       torch.float64).numpy().astype(dt)
+    f["b"] = layout.pack_spinor(g, fields.random_spinor(g, seed=seed + 3), torch.float64).numpy().astype(dt)
+    alpha = 1.0 if family in ("clover", "tm_clover") else 4.2
+    mu_t = 0.3
+    p = dict(coeff_s=kappa, coeff_t_f=kappa, coeff_t_b=kappa, alpha=alpha,
+             mu=mu_t / alpha if family == "tm" else 0.0,
+             muinv=alpha / (alpha ** 2 + mu_t ** 2) if family == "tm" else 1.0,
+             rho=0.05 if family in ("clover", "tm_clover") else 0.0, tbc_mask=0, tbc_phases=None)
+    return f, p
+
+
+def oracle_schur(g: Geometry, family, f, p, x, isign=1, target_cb=1):
+    """Mhat x (or Mhat^dag x) with the oracle: plain kernel on the other
+    checkerboard (hops scaled by 1/alpha for Wilson), achimbdpsi on target."""
+    import oracle as O
+    other = 1 - target_cb
+    sc = 1.0 / p["alpha"] if family == "wilson" else 1.0
+    clov = f["clov_dag"] if (family == "tm_clover" and isign < 0) else f["clov"]
+    q = dict(p)
+    q.pop("tbc_phases")
+    p1 = O.make_params(**dict(q, coeff_s=p["coeff_s"] * sc, coeff_t_f=p["coeff_t_f"] * sc,
+                              coeff_t_b=p["coeff_t_b"] * sc))
+    tmp = O.dslash(g, family, "dslash", isign, other, x, f["gauge"][other], clover=clov[other], params=p1)
+    p2 = O.make_params(**q)
+    return O.dslash(g, family, "achimbdpsi", isign, target_cb, tmp, f["gauge"][target_cb], chi=x,
+                    clover=clov[target_cb], params=p2)
