@@ -348,6 +348,25 @@ typedef struct qb200_operator {
 int qb200_schur_apply(const qb200_lattice *lat, const qb200_operator *op, int isign, const void *in, void *out,
                       void *tmp_other_cb, void *stream);
 
+/* Allocation-free form of qb200_schur_apply, for callers that cannot
+ * provide device scratch memory -- for example a host program whose device
+ * memory is owned entirely by its own allocator and that may not call
+ * cudaMalloc from this code path, or a time-critical loop where an
+ * allocation could synchronise the device.  It has no counterpart in the
+ * reference.  The intermediate spinor (the other checkerboard) lives in a
+ * static device array of QB200_NOALLOC_SCRATCH_BYTES (32 MiB) that every GPU
+ * loading the library holds until exit.  A lattice whose one-checkerboard
+ * spinor array (padding included) is larger -- beyond about 349,000 sites
+ * per checkerboard in FP32, 174,000 in FP64; a 24^3 x 48 FP32 lattice fits --
+ * is rejected with QB200_EINVAL.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) with that device current;
+ * make that first call before any stream capture.  All calls share the one
+ * array: calls that overlap on the GPU race and must be serialised by the
+ * caller.  The function allocates nothing. */
+#define QB200_NOALLOC_SCRATCH_BYTES (32 << 20)
+int qb200_schur_apply_noalloc(const qb200_lattice *lat, const qb200_operator *op, int isign, const void *in,
+                              void *out, void *stream);
+
 /* BLAS on n storage elements (a whole spinor array, padding included).
  * Reductions accumulate in FP64 and leave the result on the device;
  * `partials` is device scratch of qb200_blas_partials_len() doubles. */

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "qphix_b200.h"
@@ -504,6 +505,66 @@ int qb200_schur_apply(const qb200_lattice *lat, const qb200_operator *op, int is
   if (!in || !out || !tmp_other_cb) return api_fail(QB200_ENULL, "in, out and tmp must be non-NULL");
   if (in == out) return api_fail(QB200_EINVAL, "out must not alias in");
   return schur(lat, op, isign > 0, in, out, tmp_other_cb, (cudaStream_t)stream);
+}
+
+// ---- allocation-free operator application -----------------------------
+//
+// Device scratch of qb200_schur_apply_noalloc: the intermediate spinor on the
+// other checkerboard.  It is a module global, so every GPU that loads the
+// library holds these bytes until the process exits, and every call shares
+// them: calls whose work overlaps on the GPU (different streams, different
+// host threads) race on this one buffer.  Nothing in it has to start at zero:
+// the first kernel of each call writes every site of the intermediate before
+// the second kernel reads it, and padding blocks are never read.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[QB200_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+// device address of g_noalloc_scratch, looked up once per device (with that
+// device current) by the first call made on it
+void *noalloc_scratch(int *rc)
+{
+  static std::mutex mu;
+  static void *addr[128] = {nullptr};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= 128) {
+    *rc = cuda_rc(e == cudaSuccess ? cudaErrorInvalidDevice : e, "no-alloc scratch: current device");
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      *rc = cuda_rc(e == cudaSuccess ? cudaErrorInvalidSymbol : e, "no-alloc scratch: cudaGetSymbolAddress");
+      return nullptr;
+    }
+    addr[dev] = p;
+  }
+  *rc = QB200_OK;
+  return addr[dev];
+}
+} // namespace
+
+int qb200_schur_apply_noalloc(const qb200_lattice *lat, const qb200_operator *op, int isign, const void *in,
+                              void *out, void *stream)
+{
+  int rc = check_op(lat, op);
+  if (rc) return rc;
+  if (!in || !out) return api_fail(QB200_ENULL, "in and out must be non-NULL");
+  if (in == out) return api_fail(QB200_EINVAL, "out must not alias in");
+  const size_t need = spinor_bytes(lat);
+  if (need > (size_t)QB200_NOALLOC_SCRATCH_BYTES) {
+    char msg[256];
+    std::snprintf(msg, sizeof(msg),
+                  "qb200_schur_apply_noalloc: the lattice needs %zu bytes of scratch for one spinor, more than "
+                  "the %d bytes built into the library; use qb200_schur_apply with a caller buffer",
+                  need, (int)QB200_NOALLOC_SCRATCH_BYTES);
+    return api_fail(QB200_EINVAL, msg);
+  }
+  void *tmp = noalloc_scratch(&rc);
+  if (!tmp) return rc;
+  return schur(lat, op, isign > 0, in, out, tmp, (cudaStream_t)stream);
 }
 
 long long qb200_cg_workspace_bytes(const qb200_lattice *lat) { return (long long)ws_bytes(lat, 6); }

@@ -80,6 +80,7 @@ _IP = ctypes.POINTER(ctypes.c_int)
 _LL = ctypes.c_longlong
 SIGNATURES.update({
     "qb200_schur_apply": [_LAT, _OP, _I, _P, _P, _P, _P],
+    "qb200_schur_apply_noalloc": [_LAT, _OP, _I, _P, _P, _P],
     "qb200_blas_axpby": [_I, _LL, _D, _P, _D, _P, _P],
     "qb200_blas_convert": [_I, _P, _I, _P, _LL, _D, _P],
     "qb200_blas_dot": [_I, _LL, _P, _P, _P, _P, _P],
