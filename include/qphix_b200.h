@@ -39,7 +39,8 @@
  *
  * Face (halo) buffers are site-major: FT[n_face_sites][2 spin][3 colour][2 re/im],
  * the half-spinor ordering of codegen/data_types.cc:508-543 with one site per
- * entry.  Face sites are enumerated in increasing (t, z, y, xcb) order of the
+ * entry (QB200_F16N: 12 halves scaled by the site's norm, then the FP32 norm,
+ * 14 halves per site).  Face sites are enumerated in increasing (t, z, y, xcb) order of the
  * sites whose coordinate in the face dimension is 0 (back face) or N-1
  * (forward face).
  *
@@ -75,6 +76,11 @@ extern "C" {
 #define QB200_F32 0
 #define QB200_F64 1
 #define QB200_F16 2 /* IEEE binary16 bits, unscaled: the reference's `half` */
+/* FP16 spinors with a per-site FP32 norm: each FourSpinorBlock is followed by
+ * float norm[S] (block = 24*S halves + 2*S halves, values = half * norm);
+ * links and clover are plain binary16.  Not in the reference (new format). */
+#define QB200_F16N 3
+#define QB200_BF16 4 /* bfloat16 storage everywhere; not in the reference */
 
 typedef struct qb200_lattice {
   int nx, ny, nz, nt; /* local lattice extents in full sites; nx even */
@@ -82,7 +88,7 @@ typedef struct qb200_lattice {
   int veclen;         /* V: sites per gauge/clover tile; V % S == 0 */
   int pad_xy;         /* spinor blocks of padding after each xy plane */
   int pad_xyz;        /* spinor blocks of padding after each xyz volume */
-  int ftype;          /* QB200_F32 / QB200_F64 / QB200_F16 */
+  int ftype;          /* QB200_F32 / F64 / F16 / F16N / BF16 (F16N, BF16: soalen >= 4) */
   int compress12;     /* 1: gauge tiles store 2 rows (12 reals), 0: 3 rows */
   /* time boundary: hops that cross the global t edge are multiplied by
    * t_boundary (+1 periodic, -1 antiperiodic).  t_edge_lo / t_edge_hi say
@@ -378,6 +384,11 @@ int qb200_blas_dot(int ftype, long long n, const void *x, const void *y, double 
                    void *stream);
 int qb200_blas_cdot(const qb200_lattice *lat, const void *x, const void *y, double *result /* re, im */,
                     double *partials, void *stream);
+/* out = scale * in between spinor arrays of two lattices of the same shape
+ * and any storage types (the only conversion that handles QB200_F16N, whose
+ * per-site norms the element-wise qb200_blas_* calls reject) */
+int qb200_spinor_convert(const qb200_lattice *lat_out, void *out, const qb200_lattice *lat_in, const void *in,
+                         double scale, void *stream);
 
 /* Solvers for Mhat x = b on the target checkerboard.  Device workspace of
  * the size the *_workspace_bytes function returns is passed by the caller.

@@ -137,7 +137,7 @@ def face_pack(g, isign, psi_cb, psi, dir):
     L = liboracle()
     lat = lattice_struct(g)
     n = L.oracle_face_count(ctypes.byref(lat), psi_cb, dir)
-    buf = np.zeros(12 * n, dtype=psi.dtype)
+    buf = np.zeros((14 if g.ftype == 3 else 12) * n, dtype=psi.dtype)
     scratch = np.zeros(4 * n + 4, dtype=np.int32)
     rc = L.oracle_face_pack(ctypes.byref(lat), 1 if isign > 0 else -1, psi_cb, _ptr(psi), _ptr(buf), dir,
                             _ptr(scratch))

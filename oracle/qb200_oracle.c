@@ -72,12 +72,23 @@ static int make_geo(const qb200_lattice *l, geo *g)
   return 0;
 }
 
+/* elements per lane of a spinor block: 24, or 26 for F16N (24 halves plus
+ * the FP32 norm in two halves) */
+static int spb(const geo *g) { return g->ft == QB200_F16N ? 26 : 24; }
+
 /* index of component (c, s, ri) of site (xcb,y,z,t) in a spinor field */
 static long long sp_idx(const geo *g, int xcb, int y, int z, int t, int c,
                         int s, int ri)
 {
   long long blk = t * g->Pxyz + z * g->Pxy + (long long)y * g->nvecs + xcb / g->S;
-  return blk * 24 * g->S + ((c * 4 + s) * 2 + ri) * g->S + xcb % g->S;
+  return blk * spb(g) * g->S + ((c * 4 + s) * 2 + ri) * g->S + xcb % g->S;
+}
+
+/* the FP32 norm of an F16N site */
+static float *sp_norm(const geo *g, const void *f, int xcb, int y, int z, int t)
+{
+  long long blk = t * g->Pxyz + z * g->Pxy + (long long)y * g->nvecs + xcb / g->S;
+  return (float *)((const _Float16 *)f + blk * 26 * g->S + 24 * g->S) + xcb % g->S;
 }
 
 static long long tile_of(const geo *g, int xcb, int y, int z, int t)
@@ -94,12 +105,31 @@ static int lane_of(const geo *g, int xcb, int y)
 /* ------------------------------------------------------------------ */
 /* storage access                                                      */
 
+/* bfloat16: the upper 16 bits of an IEEE binary32, rounded to nearest even */
+static double bf16_to_d(uint16_t b)
+{
+  uint32_t u = (uint32_t)b << 16;
+  float f;
+  memcpy(&f, &u, 4);
+  return f;
+}
+
+static uint16_t d_to_bf16(double v)
+{
+  float f = (float)v;
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+
 static double ld(const void *p, int ft, long long i)
 {
   switch (ft) {
   case QB200_F32: return ((const float *)p)[i];
   case QB200_F64: return ((const double *)p)[i];
-  default: return (double)((const _Float16 *)p)[i];
+  case QB200_BF16: return bf16_to_d(((const uint16_t *)p)[i]);
+  default: return (double)((const _Float16 *)p)[i]; /* F16 and the halves of F16N */
   }
 }
 
@@ -108,6 +138,7 @@ static void st(void *p, int ft, long long i, double v)
   switch (ft) {
   case QB200_F32: ((float *)p)[i] = (float)v; break;
   case QB200_F64: ((double *)p)[i] = v; break;
+  case QB200_BF16: ((uint16_t *)p)[i] = d_to_bf16(v); break;
   default: ((_Float16 *)p)[i] = (_Float16)(float)v; break;
   }
 }
@@ -115,20 +146,64 @@ static void st(void *p, int ft, long long i, double v)
 static void load_spinor(const geo *g, const void *f, int xcb, int y, int z,
                         int t, cplx sp[4][3])
 {
+  double nrm = g->ft == QB200_F16N ? *sp_norm(g, f, xcb, y, z, t) : 1.0;
   for (int c = 0; c < 3; c++)
     for (int s = 0; s < 4; s++)
-      sp[s][c] = ld(f, g->ft, sp_idx(g, xcb, y, z, t, c, s, 0)) +
-                 I * ld(f, g->ft, sp_idx(g, xcb, y, z, t, c, s, 1));
+      sp[s][c] = nrm * (ld(f, g->ft, sp_idx(g, xcb, y, z, t, c, s, 0)) +
+                        I * ld(f, g->ft, sp_idx(g, xcb, y, z, t, c, s, 1)));
 }
 
 static void store_spinor(const geo *g, void *f, int xcb, int y, int z, int t,
                          cplx sp[4][3])
 {
+  double scale = 1.0;
+  if (g->ft == QB200_F16N) {
+    double m = 0.0;
+    for (int c = 0; c < 3; c++)
+      for (int s = 0; s < 4; s++) {
+        m = fmax(m, fabs(creal(sp[s][c])));
+        m = fmax(m, fabs(cimag(sp[s][c])));
+      }
+    float nrm = m > 0.0 ? (float)m : 1.0f;
+    *sp_norm(g, f, xcb, y, z, t) = nrm;
+    scale = 1.0 / nrm;
+  }
   for (int c = 0; c < 3; c++)
     for (int s = 0; s < 4; s++) {
-      st(f, g->ft, sp_idx(g, xcb, y, z, t, c, s, 0), creal(sp[s][c]));
-      st(f, g->ft, sp_idx(g, xcb, y, z, t, c, s, 1), cimag(sp[s][c]));
+      st(f, g->ft, sp_idx(g, xcb, y, z, t, c, s, 0), scale * creal(sp[s][c]));
+      st(f, g->ft, sp_idx(g, xcb, y, z, t, c, s, 1), scale * cimag(sp[s][c]));
     }
+}
+
+/* one face record: 12 values (F16N: scaled by a norm stored after them) */
+static int face_elems(const geo *g) { return g->ft == QB200_F16N ? 14 : 12; }
+
+static void store_face(const geo *g, void *buf, long long i, cplx b[2][3])
+{
+  long long o = i * face_elems(g);
+  double scale = 1.0;
+  if (g->ft == QB200_F16N) {
+    double m = 0.0;
+    for (int s = 0; s < 2; s++)
+      for (int c = 0; c < 3; c++) m = fmax(m, fmax(fabs(creal(b[s][c])), fabs(cimag(b[s][c]))));
+    float nrm = m > 0.0 ? (float)m : 1.0f;
+    *(float *)((_Float16 *)buf + o + 12) = nrm;
+    scale = 1.0 / nrm;
+  }
+  for (int s = 0; s < 2; s++)
+    for (int c = 0; c < 3; c++) {
+      st(buf, g->ft, o + (s * 3 + c) * 2 + 0, scale * creal(b[s][c]));
+      st(buf, g->ft, o + (s * 3 + c) * 2 + 1, scale * cimag(b[s][c]));
+    }
+}
+
+static void load_face(const geo *g, const void *buf, long long i, cplx b[2][3])
+{
+  long long o = i * face_elems(g);
+  double nrm = g->ft == QB200_F16N ? *(const float *)((const _Float16 *)buf + o + 12) : 1.0;
+  for (int s = 0; s < 2; s++)
+    for (int c = 0; c < 3; c++)
+      b[s][c] = nrm * (ld(buf, g->ft, o + (s * 3 + c) * 2) + I * ld(buf, g->ft, o + (s * 3 + c) * 2 + 1));
 }
 
 /* stored link G (= U^T) of direction d at an output site */
@@ -451,11 +526,7 @@ int oracle_face_pack(const qb200_lattice *lat, int isign, int psi_cb,
     cplx sp[4][3], b[2][3];
     load_spinor(&g, psi, fx[i], fy[i], fz[i], ft[i], sp);
     project(pidx, sp, b);
-    for (int s = 0; s < 2; s++)
-      for (int c = 0; c < 3; c++) {
-        st(outbuf, g.ft, i * 12 + (s * 3 + c) * 2 + 0, creal(b[s][c]));
-        st(outbuf, g.ft, i * 12 + (s * 3 + c) * 2 + 1, cimag(b[s][c]));
-      }
+    store_face(&g, outbuf, i, b);
   }
   return QB200_OK;
 }
@@ -484,10 +555,7 @@ int oracle_face_unpack(const qb200_lattice *lat, int family, int isign,
   for (long long i = 0; i < n; i++) {
     cplx o[4][3], dout[4][3], b[2][3], ub[2][3], G[3][3];
     load_spinor(&g, out, fx[i], fy[i], fz[i], ft[i], o);
-    for (int s = 0; s < 2; s++)
-      for (int c = 0; c < 3; c++)
-        b[s][c] = ld(inbuf, g.ft, i * 12 + (s * 3 + c) * 2) +
-                  I * ld(inbuf, g.ft, i * 12 + (s * 3 + c) * 2 + 1);
+    load_face(&g, inbuf, i, b);
     load_link(&g, gauge, fx[i], fy[i], fz[i], ft[i], dir, G);
     mult_link(G, isBack, b, ub);
     if (tbc) apply_tbc(!isBack, tbc_phases + 2 * dim, ub);

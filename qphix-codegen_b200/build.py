@@ -23,8 +23,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
            "-Xptxas", "-v", "--expt-relaxed-constexpr", "-I" + CSRC, "-I" + INCLUDE]
 
-FTYPES = {"f32": "float", "f64": "double", "f16": "__half"}
+FTYPES = {"f32": "float", "f64": "double", "f16": "__half", "f16n": "half_norm", "bf16": "__nv_bfloat16"}
 SOALENS = [1, 2, 4, 8, 16]
+WIDE_ONLY = ("f16n", "bf16")   # built for SOALEN 4, 8, 16
 
 
 def nvcc():
@@ -40,6 +41,8 @@ def units():
            (os.path.join(BUILD, "qb200_solver.o"), [], os.path.join(CSRC, "qb200_solver.cu"))]
     for tag, ft in FTYPES.items():
         for s in SOALENS:
+            if tag in WIDE_ONLY and s < 4:
+                continue
             out.append((os.path.join(BUILD, "inst_%s_s%d.o" % (tag, s)),
                         ["-DQB_FT=%s" % ft, "-DQB_S=%d" % s],
                         os.path.join(CSRC, "qb200_inst.cu")))

@@ -52,8 +52,11 @@ int make_geo(const qb200_lattice *l, GeoDev &g)
   const int ngy = l->veclen / l->soalen;
   if (l->ny % ngy) return fail(QB200_EINVAL, "ny = %d is not a multiple of veclen/soalen = %d", l->ny, ngy);
   if (l->pad_xy < 0 || l->pad_xyz < 0) return fail(QB200_EINVAL, "negative padding");
-  if (l->ftype != QB200_F32 && l->ftype != QB200_F64 && l->ftype != QB200_F16)
+  if (l->ftype != QB200_F32 && l->ftype != QB200_F64 && l->ftype != QB200_F16 && l->ftype != QB200_F16N &&
+      l->ftype != QB200_BF16)
     return fail(QB200_ELAYOUT, "unknown storage type %d", l->ftype);
+  if ((l->ftype == QB200_F16N || l->ftype == QB200_BF16) && l->soalen < 4)
+    return fail(QB200_ELAYOUT, "storage type %d is built for soalen 4, 8 and 16 only", l->ftype);
   const long long nsites = (long long)(l->nx / 2) * l->ny * l->nz * l->nt;
   if (nsites >= (1LL << 31)) return fail(QB200_EINVAL, "checkerboard of %lld sites is too large", nsites);
   g.nx = l->nx;
@@ -135,12 +138,12 @@ cudaError_t dispatch_body(const qb200_lattice *l, const Body &b, const GeoDev &g
   ls.fam = b.fam;
   ls.ach = b.ach;
   ls.comp12 = l->compress12 != 0;
-  const FT *psi = (const FT *)b.psi, *chi = (const FT *)b.chi, *u = (const FT *)b.gauge,
-           *cl = (const FT *)b.clov;
-  FT *out = (FT *)b.out;
+  typedef elem_t<FT> E;
+  const E *psi = (const E *)b.psi, *chi = (const E *)b.chi, *u = (const E *)b.gauge, *cl = (const E *)b.clov;
+  E *out = (E *)b.out;
   switch (l->soalen) {
-  case 1: return launch_dslash<FT, 1>(ls, psi, chi, u, cl, out, g, p, st);
-  case 2: return launch_dslash<FT, 2>(ls, psi, chi, u, cl, out, g, p, st);
+  case 1: return launch_dslash<FT, (ftraits<FT>::WIDE_ONLY ? 4 : 1)>(ls, psi, chi, u, cl, out, g, p, st);
+  case 2: return launch_dslash<FT, (ftraits<FT>::WIDE_ONLY ? 4 : 2)>(ls, psi, chi, u, cl, out, g, p, st);
   case 4: return launch_dslash<FT, 4>(ls, psi, chi, u, cl, out, g, p, st);
   case 8: return launch_dslash<FT, 8>(ls, psi, chi, u, cl, out, g, p, st);
   default: return launch_dslash<FT, 16>(ls, psi, chi, u, cl, out, g, p, st);
@@ -166,7 +169,9 @@ int run_body(const qb200_lattice *l, const Body &b, void *stream)
   switch (l->ftype) {
   case QB200_F32: e = dispatch_body<float>(l, b, g, st); break;
   case QB200_F64: e = dispatch_body<double>(l, b, g, st); break;
-  default: e = dispatch_body<__half>(l, b, g, st); break;
+  case QB200_F16: e = dispatch_body<__half>(l, b, g, st); break;
+  case QB200_F16N: e = dispatch_body<half_norm>(l, b, g, st); break;
+  default: e = dispatch_body<__nv_bfloat16>(l, b, g, st); break;
   }
   return cuda_status(e, "dslash launch");
 }
@@ -194,11 +199,12 @@ template <typename FT>
 cudaError_t dispatch_pack(const qb200_lattice *l, const void *psi, void *buf, const GeoDev &g,
                           const FaceSpec &f, int isPlus, cudaStream_t st)
 {
-  const FT *p = (const FT *)psi;
-  FT *o = (FT *)buf;
+  typedef elem_t<FT> E;
+  const E *p = (const E *)psi;
+  E *o = (E *)buf;
   switch (l->soalen) {
-  case 1: return launch_face_pack<FT, 1>(p, o, g, f, isPlus, st);
-  case 2: return launch_face_pack<FT, 2>(p, o, g, f, isPlus, st);
+  case 1: return launch_face_pack<FT, (ftraits<FT>::WIDE_ONLY ? 4 : 1)>(p, o, g, f, isPlus, st);
+  case 2: return launch_face_pack<FT, (ftraits<FT>::WIDE_ONLY ? 4 : 2)>(p, o, g, f, isPlus, st);
   case 4: return launch_face_pack<FT, 4>(p, o, g, f, isPlus, st);
   case 8: return launch_face_pack<FT, 8>(p, o, g, f, isPlus, st);
   default: return launch_face_pack<FT, 16>(p, o, g, f, isPlus, st);
@@ -223,7 +229,9 @@ int run_pack(const qb200_lattice *l, int isPlus, int psi_cb, const void *psi, vo
   switch (l->ftype) {
   case QB200_F32: e = dispatch_pack<float>(l, psi, outbuf, g, f, isPlus, st); break;
   case QB200_F64: e = dispatch_pack<double>(l, psi, outbuf, g, f, isPlus, st); break;
-  default: e = dispatch_pack<__half>(l, psi, outbuf, g, f, isPlus, st); break;
+  case QB200_F16: e = dispatch_pack<__half>(l, psi, outbuf, g, f, isPlus, st); break;
+  case QB200_F16N: e = dispatch_pack<half_norm>(l, psi, outbuf, g, f, isPlus, st); break;
+  default: e = dispatch_pack<__nv_bfloat16>(l, psi, outbuf, g, f, isPlus, st); break;
   }
   return cuda_status(e, "face pack launch");
 }
@@ -248,12 +256,13 @@ cudaError_t dispatch_unpack(const qb200_lattice *l, const Unpack &u, const GeoDe
   p.beta[0] = (C)u.beta;
   p.mu = (C)u.mu;
   p.muinv = (C)u.muinv;
-  const FT *in = (const FT *)u.inbuf, *gg = (const FT *)u.gauge, *cl = (const FT *)u.clov;
-  FT *o = (FT *)u.out;
+  typedef elem_t<FT> E;
+  const E *in = (const E *)u.inbuf, *gg = (const E *)u.gauge, *cl = (const E *)u.clov;
+  E *o = (E *)u.out;
   const bool c12 = l->compress12 != 0;
   switch (l->soalen) {
-  case 1: return launch_face_unpack<FT, 1>(u.fam, c12, in, gg, cl, o, g, f, p, st);
-  case 2: return launch_face_unpack<FT, 2>(u.fam, c12, in, gg, cl, o, g, f, p, st);
+  case 1: return launch_face_unpack<FT, (ftraits<FT>::WIDE_ONLY ? 4 : 1)>(u.fam, c12, in, gg, cl, o, g, f, p, st);
+  case 2: return launch_face_unpack<FT, (ftraits<FT>::WIDE_ONLY ? 4 : 2)>(u.fam, c12, in, gg, cl, o, g, f, p, st);
   case 4: return launch_face_unpack<FT, 4>(u.fam, c12, in, gg, cl, o, g, f, p, st);
   case 8: return launch_face_unpack<FT, 8>(u.fam, c12, in, gg, cl, o, g, f, p, st);
   default: return launch_face_unpack<FT, 16>(u.fam, c12, in, gg, cl, o, g, f, p, st);
@@ -280,7 +289,9 @@ int run_unpack(const qb200_lattice *l, const Unpack &u, void *stream)
   switch (l->ftype) {
   case QB200_F32: e = dispatch_unpack<float>(l, u, g, f, st); break;
   case QB200_F64: e = dispatch_unpack<double>(l, u, g, f, st); break;
-  default: e = dispatch_unpack<__half>(l, u, g, f, st); break;
+  case QB200_F16: e = dispatch_unpack<__half>(l, u, g, f, st); break;
+  case QB200_F16N: e = dispatch_unpack<half_norm>(l, u, g, f, st); break;
+  default: e = dispatch_unpack<__nv_bfloat16>(l, u, g, f, st); break;
   }
   return cuda_status(e, "face unpack launch");
 }
@@ -291,7 +302,7 @@ long long elem_count(const qb200_lattice *l, int what)
   if (make_geo(l, g)) return -1;
   const long long ntiles = (long long)l->nt * l->nz * g.nyg * g.nvecs;
   switch (what) {
-  case 0: return (long long)l->nt * g.Pxyz * 24 * l->soalen;
+  case 0: return (long long)l->nt * g.Pxyz * (l->ftype == QB200_F16N ? 26 : 24) * l->soalen;
   case 1: return ntiles * 8 * (l->compress12 ? 2 : 3) * 6 * l->veclen;
   case 2: return ntiles * 72 * l->veclen;
   default: return ntiles * 144 * l->veclen;
@@ -340,7 +351,9 @@ int qb200_abi_version(void) { return QB200_ABI_VERSION; }
 const char *qb200_last_error(void) { return g_err.c_str(); }
 int qb200_layout_supported(int ftype, int soalen)
 {
-  return (ftype == QB200_F32 || ftype == QB200_F64 || ftype == QB200_F16) && soalen_ok(soalen);
+  if (!soalen_ok(soalen)) return 0;
+  if (ftype == QB200_F32 || ftype == QB200_F64 || ftype == QB200_F16) return 1;
+  return (ftype == QB200_F16N || ftype == QB200_BF16) && soalen >= 4;
 }
 long long qb200_spinor_elems(const qb200_lattice *lat) { return elem_count(lat, 0); }
 long long qb200_gauge_elems(const qb200_lattice *lat) { return elem_count(lat, 1); }

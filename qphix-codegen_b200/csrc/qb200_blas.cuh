@@ -9,6 +9,7 @@
 // host synchronisation).
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -31,16 +32,27 @@ template <> struct vec16<double> {
 template <> struct vec16<__half> {
   static constexpr int n = 8;
 };
+template <> struct vec16<__nv_bfloat16> {
+  static constexpr int n = 8;
+};
 
 template <typename FT> __device__ __forceinline__ double to_d(FT v);
 template <> __device__ __forceinline__ double to_d<float>(float v) { return (double)v; }
 template <> __device__ __forceinline__ double to_d<double>(double v) { return v; }
 template <> __device__ __forceinline__ double to_d<__half>(__half v) { return (double)__half2float(v); }
+template <> __device__ __forceinline__ double to_d<__nv_bfloat16>(__nv_bfloat16 v)
+{
+  return (double)__bfloat162float(v);
+}
 
 template <typename FT> __device__ __forceinline__ FT from_d(double v);
 template <> __device__ __forceinline__ float from_d<float>(double v) { return (float)v; }
 template <> __device__ __forceinline__ double from_d<double>(double v) { return v; }
 template <> __device__ __forceinline__ __half from_d<__half>(double v) { return __float2half_rn((float)v); }
+template <> __device__ __forceinline__ __nv_bfloat16 from_d<__nv_bfloat16>(double v)
+{
+  return __float2bfloat16_rn((float)v);
+}
 
 template <typename FT> struct V16 {
   FT e[vec16<FT>::n];
@@ -189,6 +201,129 @@ __global__ void __launch_bounds__(kRedThreads) finish_kernel(const double *__res
   if (threadIdx.x == 0) {
     result[0] = a;
     if (ncomp > 1) result[1] = b;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP16 spinors with a per-site norm: blocks of 24*S halves followed by S
+// FP32 norms (2*S halves).  These kernels work per site lane: decode the 24
+// values, operate in FP64, re-encode with a fresh norm.
+
+template <int S> struct F16NSite {
+  static __device__ __forceinline__ void load(const __half *f, long long sl, double (&v)[24])
+  {
+    const long long blk = sl / S;
+    const int l = (int)(sl - blk * S);
+    const __half *b = f + blk * 26 * S;
+    const double nrm = (double)__ldg(reinterpret_cast<const float *>(b + 24 * S) + l);
+#pragma unroll
+    for (int k = 0; k < 24; k++) v[k] = (double)__half2float(b[k * S + l]) * nrm;
+  }
+  static __device__ __forceinline__ void store(__half *f, long long sl, const double (&v)[24])
+  {
+    const long long blk = sl / S;
+    const int l = (int)(sl - blk * S);
+    __half *b = f + blk * 26 * S;
+    double m = 0.0;
+#pragma unroll
+    for (int k = 0; k < 24; k++) m = fmax(m, fabs(v[k]));
+    const float nrm = m > 0.0 ? (float)m : 1.0f;
+    reinterpret_cast<float *>(b + 24 * S)[l] = nrm;
+    const double inv = 1.0 / (double)nrm;
+#pragma unroll
+    for (int k = 0; k < 24; k++) b[k * S + l] = __float2half_rn((float)(v[k] * inv));
+  }
+};
+
+// y = a x + b y
+template <int S>
+__global__ void __launch_bounds__(256) axpby_f16n_kernel(long long nsl, ScalarRef a, const __half *__restrict__ x,
+                                                         ScalarRef b, __half *__restrict__ y)
+{
+  const double av = a.get(), bv = b.get();
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nsl;
+       i += (long long)gridDim.x * blockDim.x) {
+    double vx[24], vy[24];
+    F16NSite<S>::load(x, i, vx);
+    F16NSite<S>::load(y, i, vy);
+#pragma unroll
+    for (int k = 0; k < 24; k++) vy[k] = av * vx[k] + bv * vy[k];
+    F16NSite<S>::store(y, i, vy);
+  }
+}
+
+// complex y = a x + b y (components 2j, 2j+1 are re, im)
+template <int S>
+__global__ void __launch_bounds__(256) caxpby_f16n_kernel(long long nsl, double ar, double ai,
+                                                          const __half *__restrict__ x, double br, double bi,
+                                                          __half *__restrict__ y)
+{
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nsl;
+       i += (long long)gridDim.x * blockDim.x) {
+    double vx[24], vy[24];
+    F16NSite<S>::load(x, i, vx);
+    F16NSite<S>::load(y, i, vy);
+#pragma unroll
+    for (int j = 0; j < 12; j++) {
+      const double xr = vx[2 * j], xi = vx[2 * j + 1], yr = vy[2 * j], yi = vy[2 * j + 1];
+      vy[2 * j] = ar * xr - ai * xi + br * yr - bi * yi;
+      vy[2 * j + 1] = ar * xi + ai * xr + br * yi + bi * yr;
+    }
+    F16NSite<S>::store(y, i, vy);
+  }
+}
+
+// partials: real dot (CPLX = false) or complex <x, y> (CPLX = true)
+template <int S, bool CPLX>
+__global__ void __launch_bounds__(kRedThreads) dot_f16n_partial_kernel(long long nsl, const __half *__restrict__ x,
+                                                                       const __half *__restrict__ y,
+                                                                       double *__restrict__ partials)
+{
+  double re = 0.0, im = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nsl;
+       i += (long long)gridDim.x * blockDim.x) {
+    double vx[24], vy[24];
+    F16NSite<S>::load(x, i, vx);
+    F16NSite<S>::load(y, i, vy);
+    if (CPLX) {
+#pragma unroll
+      for (int j = 0; j < 12; j++) {
+        re += vx[2 * j] * vy[2 * j] + vx[2 * j + 1] * vy[2 * j + 1];
+        im += vx[2 * j] * vy[2 * j + 1] - vx[2 * j + 1] * vy[2 * j];
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 24; k++) re += vx[k] * vy[k];
+    }
+  }
+  block_sum2(re, im);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = re;
+    partials[kRedBlocks + blockIdx.x] = im;
+  }
+}
+
+// between F16N and a plain storage type FP (24*S elements per block)
+template <int S, typename FP, bool TO_F16N>
+__global__ void __launch_bounds__(256) convert_f16n_kernel(long long nsl, double scale, const void *__restrict__ in,
+                                                           void *__restrict__ out)
+{
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nsl;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long blk = i / S;
+    const int l = (int)(i - blk * S);
+    double v[24];
+    if (TO_F16N) {
+      const FP *p = reinterpret_cast<const FP *>(in) + blk * 24 * S + l;
+#pragma unroll
+      for (int k = 0; k < 24; k++) v[k] = scale * to_d(p[k * S]);
+      F16NSite<S>::store(reinterpret_cast<__half *>(out), i, v);
+    } else {
+      F16NSite<S>::load(reinterpret_cast<const __half *>(in), i, v);
+      FP *p = reinterpret_cast<FP *>(out) + blk * 24 * S + l;
+#pragma unroll
+      for (int k = 0; k < 24; k++) p[k * S] = from_d<FP>(scale * v[k]);
+    }
   }
 }
 

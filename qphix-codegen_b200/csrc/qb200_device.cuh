@@ -15,6 +15,7 @@
 //   - *_mbeta == *_pbeta with beta -> -beta, folded into the coefficient.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <stdint.h>
 
@@ -24,24 +25,60 @@ namespace qb200 {
 enum { FAM_WILSON = 0, FAM_CLOVER = 1, FAM_TM = 2, FAM_TMCLOV = 3 };
 
 // ---------------------------------------------------------------------
-// storage traits: FT is the storage type, C the arithmetic type
+// storage traits.  FT names the storage format, E the element type in
+// memory, C the arithmetic type; SPB is the number of E elements per site
+// lane of a spinor block (24, or 26 when two extra halves hold the site's
+// FP32 norm) and FACE the elements per face site.
+
+// FP16 spinors scaled by a per-site FP32 norm (links and clover plain FP16):
+// block = FT[3][4][2][S] halves followed by float norm[S].  WIDE_ONLY types
+// are built for SOALEN 4, 8 and 16 only.
+struct half_norm {};
 
 template <typename FT> struct ftraits;
 template <> struct ftraits<float> {
+  typedef float E;
   typedef float C;
+  static constexpr int SPB = 24, FACE = 12;
+  static constexpr bool WIDE_ONLY = false;
   static __device__ __forceinline__ float ld(const float *p) { return __ldg(p); }
   static __device__ __forceinline__ void st(float *p, float v) { *p = v; }
 };
 template <> struct ftraits<double> {
+  typedef double E;
   typedef double C;
+  static constexpr int SPB = 24, FACE = 12;
+  static constexpr bool WIDE_ONLY = false;
   static __device__ __forceinline__ double ld(const double *p) { return __ldg(p); }
   static __device__ __forceinline__ void st(double *p, double v) { *p = v; }
 };
 template <> struct ftraits<__half> {
+  typedef __half E;
   typedef float C;
+  static constexpr int SPB = 24, FACE = 12;
+  static constexpr bool WIDE_ONLY = false;
   static __device__ __forceinline__ float ld(const __half *p) { return __half2float(__ldg(p)); }
   static __device__ __forceinline__ void st(__half *p, float v) { *p = __float2half_rn(v); }
 };
+template <> struct ftraits<__nv_bfloat16> {
+  typedef __nv_bfloat16 E;
+  typedef float C;
+  static constexpr int SPB = 24, FACE = 12;
+  static constexpr bool WIDE_ONLY = true;
+  static __device__ __forceinline__ float ld(const __nv_bfloat16 *p) { return __bfloat162float(__ldg(p)); }
+  static __device__ __forceinline__ void st(__nv_bfloat16 *p, float v) { *p = __float2bfloat16_rn(v); }
+};
+template <> struct ftraits<half_norm> {
+  typedef __half E;
+  typedef float C;
+  static constexpr int SPB = 26, FACE = 14;
+  static constexpr bool WIDE_ONLY = true;
+  static __device__ __forceinline__ float ld(const __half *p) { return __half2float(__ldg(p)); }
+  static __device__ __forceinline__ void st(__half *p, float v) { *p = __float2half_rn(v); }
+};
+
+template <typename FT> using elem_t = typename ftraits<FT>::E;
+template <typename FT> using comp_t = typename ftraits<FT>::C;
 
 template <typename C> struct cx {
   C re, im;
@@ -153,11 +190,11 @@ __device__ __forceinline__ Site neighbour(const GeoDev &g, const Site &s, bool *
 
 // element index of component 0 of the site in a spinor field (add
 // ((c*4+s)*2+ri)*S for component (c,s,ri))
-template <int S>
+template <typename FT, int S>
 __device__ __forceinline__ long long spinor_base(const GeoDev &g, const Site &s)
 {
   long long blk = s.t * g.Pxyz + s.z * g.Pxy + (long long)s.y * g.nvecs + s.xcb / S;
-  return blk * (24 * S) + (s.xcb % S);
+  return blk * (ftraits<FT>::SPB * S) + (s.xcb % S);
 }
 
 // tile index and lane of a site in the gauge / clover fields
@@ -173,8 +210,8 @@ __device__ __forceinline__ long long tile_of(const GeoDev &g, const Site &s, int
 // loads
 
 template <typename FT, int S>
-__device__ __forceinline__ void load_spinor(const FT *__restrict__ f, long long base,
-                                            cx<typename ftraits<FT>::C> (&sp)[4][3])
+__device__ __forceinline__ void load_spinor(const elem_t<FT> *__restrict__ f, long long base,
+                                            cx<comp_t<FT>> (&sp)[4][3])
 {
 #pragma unroll
   for (int c = 0; c < 3; c++)
@@ -183,25 +220,48 @@ __device__ __forceinline__ void load_spinor(const FT *__restrict__ f, long long 
       sp[s][c].re = ftraits<FT>::ld(f + base + ((c * 4 + s) * 2 + 0) * S);
       sp[s][c].im = ftraits<FT>::ld(f + base + ((c * 4 + s) * 2 + 1) * S);
     }
+  if (ftraits<FT>::SPB == 26) {
+    // the lane's norm: float at half offset block*26S + 24S + 2*lane = base + 24S + lane
+    const float nrm = __ldg(reinterpret_cast<const float *>(f + base + 24 * S + (base % S)));
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+      for (int s = 0; s < 4; s++) {
+        sp[s][c].re *= nrm;
+        sp[s][c].im *= nrm;
+      }
+  }
 }
 
 template <typename FT, int S>
-__device__ __forceinline__ void store_spinor(FT *__restrict__ f, long long base,
-                                             const cx<typename ftraits<FT>::C> (&sp)[4][3])
+__device__ __forceinline__ void store_spinor(elem_t<FT> *__restrict__ f, long long base,
+                                             const cx<comp_t<FT>> (&sp)[4][3])
 {
+  typedef comp_t<FT> C;
+  C scale = (C)1;
+  if (ftraits<FT>::SPB == 26) {
+    C m = 0;
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+      for (int s = 0; s < 4; s++) m = fmax(m, fmax(fabs(sp[s][c].re), fabs(sp[s][c].im)));
+    const C nrm = m > (C)0 ? m : (C)1;
+    *reinterpret_cast<float *>(f + base + 24 * S + (base % S)) = (float)nrm;
+    scale = (C)1 / nrm;
+  }
 #pragma unroll
   for (int c = 0; c < 3; c++)
 #pragma unroll
     for (int s = 0; s < 4; s++) {
-      ftraits<FT>::st(f + base + ((c * 4 + s) * 2 + 0) * S, sp[s][c].re);
-      ftraits<FT>::st(f + base + ((c * 4 + s) * 2 + 1) * S, sp[s][c].im);
+      ftraits<FT>::st(f + base + ((c * 4 + s) * 2 + 0) * S, sp[s][c].re * scale);
+      ftraits<FT>::st(f + base + ((c * 4 + s) * 2 + 1) * S, sp[s][c].im * scale);
     }
 }
 
 // stored link G (= U^T) of direction D; `base` = tile*(8*R*6*V) + lane
 template <typename FT, bool COMP12, int D>
-__device__ __forceinline__ void load_link(const FT *__restrict__ u, long long base, int V,
-                                          cx<typename ftraits<FT>::C> (&G)[3][3])
+__device__ __forceinline__ void load_link(const elem_t<FT> *__restrict__ u, long long base, int V,
+                                          cx<comp_t<FT>> (&G)[3][3])
 {
   constexpr int R = COMP12 ? 2 : 3;
 #pragma unroll
@@ -326,12 +386,12 @@ __device__ __forceinline__ void recons(const cx<C> (&ub)[2][3], C beta, C tau, c
 // res[block rows] (+)= A in, A the Hermitian CloverBlock block `blk`
 // (dslash_common.cc:1098-1186).  base = tile*72*V + lane.
 template <typename FT, bool ACC>
-__device__ __forceinline__ void clover_block(const FT *__restrict__ cl, long long base, int V, int blk,
+__device__ __forceinline__ void clover_block(const elem_t<FT> *__restrict__ cl, long long base, int V, int blk,
                                              const cx<typename ftraits<FT>::C> (&in)[4][3],
                                              cx<typename ftraits<FT>::C> (&res)[4][3])
 {
   typedef typename ftraits<FT>::C C;
-  const FT *p = cl + base + (long long)blk * 36 * V;
+  const elem_t<FT> *p = cl + base + (long long)blk * 36 * V;
   C dg[6];
   cx<C> od[15];
 #pragma unroll
@@ -377,12 +437,12 @@ __device__ __forceinline__ void clover_block(const FT *__restrict__ cl, long lon
 // res (+)= F in, F a dense FullCloverBlock block (dslash_common.cc:1188-1232).
 // base = tile*144*V + lane.
 template <typename FT, bool ACC>
-__device__ __forceinline__ void full_clover_block(const FT *__restrict__ cl, long long base, int V, int blk,
+__device__ __forceinline__ void full_clover_block(const elem_t<FT> *__restrict__ cl, long long base, int V, int blk,
                                                   const cx<typename ftraits<FT>::C> (&in)[4][3],
                                                   cx<typename ftraits<FT>::C> (&res)[4][3])
 {
   typedef typename ftraits<FT>::C C;
-  const FT *p = cl + base + (long long)blk * 72 * V;
+  const elem_t<FT> *p = cl + base + (long long)blk * 72 * V;
 #pragma unroll
   for (int r = 0; r < 6; r++) {
     C re = 0, im = 0;

@@ -56,30 +56,64 @@ __device__ __forceinline__ Site face_site(const GeoDev &g, const FaceDev &f, int
   return s;
 }
 
-template <typename FT, int S, int D>
-__device__ __forceinline__ void pack_one(const FT *__restrict__ psi, FT *__restrict__ buf,
-                                         const GeoDev &g, const FaceDev &f, int isPlus, int i)
+// one face site: 12 values; with a per-site norm (FACE == 14) the values are
+// stored divided by the norm and the FP32 norm follows in the last two halves
+template <typename FT>
+__device__ __forceinline__ void store_face(elem_t<FT> *o, const cx<comp_t<FT>> (&b)[2][3])
 {
-  typedef typename ftraits<FT>::C C;
-  const Site s = face_site(g, f, i);
-  cx<C> sp[4][3], b[2][3];
-  load_spinor<FT, S>(psi, spinor_base<S>(g, s), sp);
-  // proj_ops_plus[D^1] for plus == proj_ops_plus[D] with sigma = -1
-  project<C, D>(sp, isPlus ? (C)-1 : (C)1, b);
-  FT *o = buf + (long long)i * 12;
+  typedef comp_t<FT> C;
+  C scale = (C)1;
+  if (ftraits<FT>::FACE == 14) {
+    C m = 0;
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) m = fmax(m, fmax(fabs(b[h][c].re), fabs(b[h][c].im)));
+    const C nrm = m > (C)0 ? m : (C)1;
+    *reinterpret_cast<float *>(o + 12) = (float)nrm;
+    scale = (C)1 / nrm;
+  }
 #pragma unroll
   for (int h = 0; h < 2; h++)
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      ftraits<FT>::st(o + (h * 3 + c) * 2 + 0, b[h][c].re);
-      ftraits<FT>::st(o + (h * 3 + c) * 2 + 1, b[h][c].im);
+      ftraits<FT>::st(o + (h * 3 + c) * 2 + 0, b[h][c].re * scale);
+      ftraits<FT>::st(o + (h * 3 + c) * 2 + 1, b[h][c].im * scale);
     }
+}
+
+template <typename FT>
+__device__ __forceinline__ void load_face(const elem_t<FT> *in, cx<comp_t<FT>> (&b)[2][3])
+{
+  typedef comp_t<FT> C;
+  C nrm = (C)1;
+  if (ftraits<FT>::FACE == 14) nrm = __ldg(reinterpret_cast<const float *>(in + 12));
+#pragma unroll
+  for (int h = 0; h < 2; h++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      b[h][c].re = ftraits<FT>::ld(in + (h * 3 + c) * 2 + 0) * nrm;
+      b[h][c].im = ftraits<FT>::ld(in + (h * 3 + c) * 2 + 1) * nrm;
+    }
+}
+
+template <typename FT, int S, int D>
+__device__ __forceinline__ void pack_one(const elem_t<FT> *__restrict__ psi, elem_t<FT> *__restrict__ buf,
+                                         const GeoDev &g, const FaceDev &f, int isPlus, int i)
+{
+  typedef comp_t<FT> C;
+  const Site s = face_site(g, f, i);
+  cx<C> sp[4][3], b[2][3];
+  load_spinor<FT, S>(psi, spinor_base<FT, S>(g, s), sp);
+  // proj_ops_plus[D^1] for plus == proj_ops_plus[D] with sigma = -1
+  project<C, D>(sp, isPlus ? (C)-1 : (C)1, b);
+  store_face<FT>(buf + (long long)i * ftraits<FT>::FACE, b);
 }
 
 template <typename FT, int S>
 __global__ void __launch_bounds__(128)
-    face_pack_kernel(const FT *__restrict__ psi, FT *__restrict__ buf, const GeoDev g, const FaceDev f,
-                     int isPlus)
+    face_pack_kernel(const elem_t<FT> *__restrict__ psi, elem_t<FT> *__restrict__ buf, const GeoDev g,
+                     const FaceDev f, int isPlus)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= f.nface) return;
@@ -96,8 +130,9 @@ __global__ void __launch_bounds__(128)
 }
 
 template <typename FT, int S, bool COMP12, int FAM, int D>
-__device__ __forceinline__ void unpack_one(const FT *__restrict__ buf, const FT *__restrict__ gauge,
-                                           const FT *__restrict__ clov, FT *__restrict__ out,
+__device__ __forceinline__ void unpack_one(const elem_t<FT> *__restrict__ buf,
+                                           const elem_t<FT> *__restrict__ gauge,
+                                           const elem_t<FT> *__restrict__ clov, elem_t<FT> *__restrict__ out,
                                            const GeoDev &g, const FaceDev &f,
                                            const OpDev<typename ftraits<FT>::C> &p, int i)
 {
@@ -110,18 +145,11 @@ __device__ __forceinline__ void unpack_one(const FT *__restrict__ buf, const FT 
   int lane;
   const long long tile = tile_of<S>(g, s, &lane);
   constexpr int R = COMP12 ? 2 : 3;
-  const long long obase = spinor_base<S>(g, s);
+  const long long obase = spinor_base<FT, S>(g, s);
 
   cx<C> o[4][3], b[2][3], ub[2][3], G[3][3];
   load_spinor<FT, S>(out, obase, o);
-  const FT *in = buf + (long long)i * 12;
-#pragma unroll
-  for (int h = 0; h < 2; h++)
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-      b[h][c].re = ftraits<FT>::ld(in + (h * 3 + c) * 2 + 0);
-      b[h][c].im = ftraits<FT>::ld(in + (h * 3 + c) * 2 + 1);
-    }
+  load_face<FT>(buf + (long long)i * ftraits<FT>::FACE, b);
   load_link<FT, COMP12, D>(gauge, tile * (8LL * R * 6 * g.V) + lane, g.V, G);
   mult_link<C, BACK>(G, b, ub);
   if ((p.tbc_mask >> MU) & 1u) {
@@ -156,8 +184,9 @@ __device__ __forceinline__ void unpack_one(const FT *__restrict__ buf, const FT 
 
 template <typename FT, int S, bool COMP12, int FAM>
 __global__ void __launch_bounds__(128)
-    face_unpack_kernel(const FT *__restrict__ buf, const FT *__restrict__ gauge, const FT *__restrict__ clov,
-                       FT *__restrict__ out, const GeoDev g, const FaceDev f,
+    face_unpack_kernel(const elem_t<FT> *__restrict__ buf, const elem_t<FT> *__restrict__ gauge,
+                       const elem_t<FT> *__restrict__ clov, elem_t<FT> *__restrict__ out, const GeoDev g,
+                       const FaceDev f,
                        const OpDev<typename ftraits<FT>::C> p)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -43,8 +43,8 @@ cudaError_t go_fam(const LaunchSpec &ls, const KArgs<FT> &a, const GeoDev &g,
 }
 
 template <typename FT, int S, bool COMP12, int FAM>
-cudaError_t go_unpack(const FT *buf, const FT *gauge, const FT *clov, FT *out, const GeoDev &g,
-                      const FaceDev &f, const OpDev<typename ftraits<FT>::C> &p, cudaStream_t st)
+cudaError_t go_unpack(const elem_t<FT> *buf, const elem_t<FT> *gauge, const elem_t<FT> *clov, elem_t<FT> *out,
+                      const GeoDev &g, const FaceDev &f, const OpDev<comp_t<FT>> &p, cudaStream_t st)
 {
   const int blocks = (f.nface + kThreads - 1) / kThreads;
   face_unpack_kernel<FT, S, COMP12, FAM><<<blocks, kThreads, 0, st>>>(buf, gauge, clov, out, g, f, p);
@@ -65,9 +65,9 @@ FaceDev to_dev(const FaceSpec &s)
 } // namespace
 
 template <typename FT, int S>
-cudaError_t launch_dslash(const LaunchSpec &ls, const FT *psi, const FT *chi, const FT *gauge,
-                          const FT *clov, FT *out, const GeoDev &g,
-                          const OpDev<typename ftraits<FT>::C> &p, cudaStream_t st)
+cudaError_t launch_dslash(const LaunchSpec &ls, const elem_t<FT> *psi, const elem_t<FT> *chi,
+                          const elem_t<FT> *gauge, const elem_t<FT> *clov, elem_t<FT> *out, const GeoDev &g,
+                          const OpDev<comp_t<FT>> &p, cudaStream_t st)
 {
   KArgs<FT> a;
   a.psi = psi;
@@ -80,8 +80,8 @@ cudaError_t launch_dslash(const LaunchSpec &ls, const FT *psi, const FT *chi, co
 }
 
 template <typename FT, int S>
-cudaError_t launch_face_pack(const FT *psi, FT *buf, const GeoDev &g, const FaceSpec &fs, int isPlus,
-                             cudaStream_t st)
+cudaError_t launch_face_pack(const elem_t<FT> *psi, elem_t<FT> *buf, const GeoDev &g, const FaceSpec &fs,
+                             int isPlus, cudaStream_t st)
 {
   if (fs.nface == 0) return cudaSuccess;
   const FaceDev f = to_dev(fs);
@@ -91,9 +91,9 @@ cudaError_t launch_face_pack(const FT *psi, FT *buf, const GeoDev &g, const Face
 }
 
 template <typename FT, int S>
-cudaError_t launch_face_unpack(int fam, bool comp12, const FT *buf, const FT *gauge, const FT *clov,
-                               FT *out, const GeoDev &g, const FaceSpec &fs,
-                               const OpDev<typename ftraits<FT>::C> &p, cudaStream_t st)
+cudaError_t launch_face_unpack(int fam, bool comp12, const elem_t<FT> *buf, const elem_t<FT> *gauge,
+                               const elem_t<FT> *clov, elem_t<FT> *out, const GeoDev &g, const FaceSpec &fs,
+                               const OpDev<comp_t<FT>> &p, cudaStream_t st)
 {
   if (fs.nface == 0) return cudaSuccess;
   const FaceDev f = to_dev(fs);
@@ -110,14 +110,14 @@ cudaError_t launch_face_unpack(int fam, bool comp12, const FT *buf, const FT *ga
   return cudaErrorInvalidValue;
 }
 
-template cudaError_t launch_dslash<QB_FT, QB_S>(const LaunchSpec &, const QB_FT *, const QB_FT *,
-                                                const QB_FT *, const QB_FT *, QB_FT *, const GeoDev &,
-                                                const OpDev<ftraits<QB_FT>::C> &, cudaStream_t);
-template cudaError_t launch_face_pack<QB_FT, QB_S>(const QB_FT *, QB_FT *, const GeoDev &,
-                                                   const FaceSpec &, int, cudaStream_t);
-template cudaError_t launch_face_unpack<QB_FT, QB_S>(int, bool, const QB_FT *, const QB_FT *,
-                                                     const QB_FT *, QB_FT *, const GeoDev &,
-                                                     const FaceSpec &, const OpDev<ftraits<QB_FT>::C> &,
+typedef elem_t<QB_FT> QB_E;
+template cudaError_t launch_dslash<QB_FT, QB_S>(const LaunchSpec &, const QB_E *, const QB_E *, const QB_E *,
+                                                const QB_E *, QB_E *, const GeoDev &, const OpDev<comp_t<QB_FT>> &,
+                                                cudaStream_t);
+template cudaError_t launch_face_pack<QB_FT, QB_S>(const QB_E *, QB_E *, const GeoDev &, const FaceSpec &, int,
+                                                   cudaStream_t);
+template cudaError_t launch_face_unpack<QB_FT, QB_S>(int, bool, const QB_E *, const QB_E *, const QB_E *, QB_E *,
+                                                     const GeoDev &, const FaceSpec &, const OpDev<comp_t<QB_FT>> &,
                                                      cudaStream_t);
 
 } // namespace qb200

@@ -18,20 +18,20 @@ struct LaunchSpec {
 
 // body kernel launcher, defined in qb200_inst.cu for each (FT, S)
 template <typename FT, int S>
-cudaError_t launch_dslash(const LaunchSpec &ls, const FT *psi, const FT *chi, const FT *gauge,
-                          const FT *clov, FT *out, const GeoDev &g,
-                          const OpDev<typename ftraits<FT>::C> &p, cudaStream_t st);
+cudaError_t launch_dslash(const LaunchSpec &ls, const elem_t<FT> *psi, const elem_t<FT> *chi,
+                          const elem_t<FT> *gauge, const elem_t<FT> *clov, elem_t<FT> *out, const GeoDev &g,
+                          const OpDev<comp_t<FT>> &p, cudaStream_t st);
 
 // face launchers, defined in qb200_inst.cu for each (FT, S)
 struct FaceSpec {
   int dir, mu, coord, par, nface, cb;
 };
 template <typename FT, int S>
-cudaError_t launch_face_pack(const FT *psi, FT *buf, const GeoDev &g, const FaceSpec &f, int isPlus,
-                             cudaStream_t st);
+cudaError_t launch_face_pack(const elem_t<FT> *psi, elem_t<FT> *buf, const GeoDev &g, const FaceSpec &f,
+                             int isPlus, cudaStream_t st);
 template <typename FT, int S>
-cudaError_t launch_face_unpack(int fam, bool comp12, const FT *buf, const FT *gauge, const FT *clov,
-                               FT *out, const GeoDev &g, const FaceSpec &f,
-                               const OpDev<typename ftraits<FT>::C> &p, cudaStream_t st);
+cudaError_t launch_face_unpack(int fam, bool comp12, const elem_t<FT> *buf, const elem_t<FT> *gauge,
+                               const elem_t<FT> *clov, elem_t<FT> *out, const GeoDev &g, const FaceSpec &f,
+                               const OpDev<comp_t<FT>> &p, cudaStream_t st);
 
 } // namespace qb200

@@ -12,11 +12,11 @@
 namespace qb200 {
 
 template <typename FT> struct KArgs {
-  const FT *psi;
-  const FT *chi;
-  const FT *gauge;
-  const FT *clov;
-  FT *out;
+  const elem_t<FT> *psi;
+  const elem_t<FT> *chi;
+  const elem_t<FT> *gauge;
+  const elem_t<FT> *clov;
+  elem_t<FT> *out;
 };
 
 template <typename FT, int S, bool COMP12, int D>
@@ -36,7 +36,7 @@ __device__ __forceinline__ void do_hop(const KArgs<FT> &a, const GeoDev &g,
   if (D == 7 && s.t == g.nt - 1 && p.t_edge_hi) beta *= p.tbound;
 
   cx<C> psi[4][3], b[2][3], ub[2][3], G[3][3];
-  load_spinor<FT, S>(a.psi, spinor_base<S>(g, n), psi);
+  load_spinor<FT, S>(a.psi, spinor_base<FT, S>(g, n), psi);
   const C sigma = p.isPlus ? (C)1 : (C)-1;
   project<C, D>(psi, sigma, b);
   load_link<FT, COMP12, D>(a.gauge, gbase, g.V, G);
@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(128)
   const long long tile = tile_of<S>(g, s, &lane);
   constexpr int R = COMP12 ? 2 : 3;
   const long long gbase = tile * (8LL * R * 6 * g.V) + lane;
-  const long long obase = spinor_base<S>(g, s);
+  const long long obase = spinor_base<FT, S>(g, s);
 
   cx<C> res[4][3];
   cx<C> acc[4][3];

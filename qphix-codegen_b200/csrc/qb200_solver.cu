@@ -38,7 +38,10 @@ int cuda_rc(cudaError_t e, const char *what)
   return api_fail(QB200_ECUDA, m.c_str());
 }
 
-int ft_bytes(int ft) { return ft == QB200_F64 ? 8 : ft == QB200_F32 ? 4 : ft == QB200_F16 ? 2 : 0; }
+int ft_bytes(int ft)
+{
+  return ft == QB200_F64 ? 8 : ft == QB200_F32 ? 4 : (ft == QB200_F16 || ft == QB200_F16N || ft == QB200_BF16) ? 2 : 0;
+}
 
 int grid_for(long long nv)
 {
@@ -62,6 +65,7 @@ cudaError_t axpby(int ft, long long n, ScalarRef a, const void *x, ScalarRef b, 
   switch (ft) {
   case QB200_F32: return axpby_t<float>(n, a, x, b, y, st);
   case QB200_F64: return axpby_t<double>(n, a, x, b, y, st);
+  case QB200_BF16: return axpby_t<__nv_bfloat16>(n, a, x, b, y, st);
   default: return axpby_t<__half>(n, a, x, b, y, st);
   }
 }
@@ -99,6 +103,7 @@ cudaError_t convert_from(int ft_in, long long n, double scale, const void *in, v
   switch (ft_in) {
   case QB200_F32: return convert_t<FO, float>(n, scale, in, out, st);
   case QB200_F64: return convert_t<FO, double>(n, scale, in, out, st);
+  case QB200_BF16: return convert_t<FO, __nv_bfloat16>(n, scale, in, out, st);
   default: return convert_t<FO, __half>(n, scale, in, out, st);
   }
 }
@@ -108,6 +113,7 @@ cudaError_t convert(int ft_out, void *out, int ft_in, const void *in, long long 
   switch (ft_out) {
   case QB200_F32: return convert_from<float>(ft_in, n, scale, in, out, st);
   case QB200_F64: return convert_from<double>(ft_in, n, scale, in, out, st);
+  case QB200_BF16: return convert_from<__nv_bfloat16>(ft_in, n, scale, in, out, st);
   default: return convert_from<__half>(ft_in, n, scale, in, out, st);
   }
 }
@@ -128,6 +134,7 @@ cudaError_t dot(int ft, long long n, const void *x, const void *y, double *parti
   switch (ft) {
   case QB200_F32: return dot_t<float>(n, x, y, partials, result, st);
   case QB200_F64: return dot_t<double>(n, x, y, partials, result, st);
+  case QB200_BF16: return dot_t<__nv_bfloat16>(n, x, y, partials, result, st);
   default: return dot_t<__half>(n, x, y, partials, result, st);
   }
 }
@@ -159,6 +166,7 @@ cudaError_t cdot(int ft, int soalen, long long n, const void *x, const void *y, 
   switch (ft) {
   case QB200_F32: return cdot_t<float>(soalen, n, x, y, partials, result, st);
   case QB200_F64: return cdot_t<double>(soalen, n, x, y, partials, result, st);
+  case QB200_BF16: return cdot_t<__nv_bfloat16>(soalen, n, x, y, partials, result, st);
   default: return cdot_t<__half>(soalen, n, x, y, partials, result, st);
   }
 }
@@ -202,8 +210,112 @@ cudaError_t caxpby(int ft, int soalen, long long n, double ar, double ai, const 
   switch (ft) {
   case QB200_F32: return caxpby_t<float>(soalen, n, ar, ai, x, br, bi, y, st);
   case QB200_F64: return caxpby_t<double>(soalen, n, ar, ai, x, br, bi, y, st);
+  case QB200_BF16: return caxpby_t<__nv_bfloat16>(soalen, n, ar, ai, x, br, bi, y, st);
   default: return caxpby_t<__half>(soalen, n, ar, ai, x, br, bi, y, st);
   }
+}
+
+// ---- vector spaces: a storage type on a lattice ----------------------------
+// F16N spinors carry per-site norms, so their BLAS works per site lane and
+// needs SOALEN; every other type is handled element-wise.
+
+struct VS {
+  int ft, S;
+  long long n; // storage elements of one spinor array
+  long long site_lanes() const { return n / (26LL * S) * S; }
+};
+
+VS vs_of(const qb200_lattice *l)
+{
+  VS v;
+  v.ft = l->ftype;
+  v.S = l->soalen;
+  v.n = qb200_spinor_elems(l);
+  return v;
+}
+
+#define QB_F16N_S(S, CALL)                                                                                        \
+  switch (S) {                                                                                                    \
+  case 4: { constexpr int SS = 4; CALL; } break;                                                                  \
+  case 8: { constexpr int SS = 8; CALL; } break;                                                                  \
+  default: { constexpr int SS = 16; CALL; } break;                                                                \
+  }
+
+cudaError_t axpby(const VS &v, ScalarRef a, const void *x, ScalarRef b, void *y, cudaStream_t st)
+{
+  if (v.ft != QB200_F16N) return axpby(v.ft, v.n, a, x, b, y, st);
+  const long long nsl = v.site_lanes();
+  QB_F16N_S(v.S, (axpby_f16n_kernel<SS><<<grid_for(nsl), 256, 0, st>>>(nsl, a, (const __half *)x, b, (__half *)y)));
+  return cudaGetLastError();
+}
+
+cudaError_t caxpby(const VS &v, double ar, double ai, const void *x, double br, double bi, void *y, cudaStream_t st)
+{
+  if (v.ft != QB200_F16N) return caxpby(v.ft, v.S, v.n, ar, ai, x, br, bi, y, st);
+  const long long nsl = v.site_lanes();
+  QB_F16N_S(v.S, (caxpby_f16n_kernel<SS><<<grid_for(nsl), 256, 0, st>>>(nsl, ar, ai, (const __half *)x, br, bi,
+                                                                          (__half *)y)));
+  return cudaGetLastError();
+}
+
+cudaError_t f16n_dot(const VS &v, bool cplx, const void *x, const void *y, double *partials, double *result,
+                     cudaStream_t st)
+{
+  const long long nsl = v.site_lanes();
+  if (cplx) {
+    QB_F16N_S(v.S, (dot_f16n_partial_kernel<SS, true><<<kRedBlocks, kRedThreads, 0, st>>>(
+                        nsl, (const __half *)x, (const __half *)y, partials)));
+  } else {
+    QB_F16N_S(v.S, (dot_f16n_partial_kernel<SS, false><<<kRedBlocks, kRedThreads, 0, st>>>(
+                        nsl, (const __half *)x, (const __half *)y, partials)));
+  }
+  finish_kernel<<<1, kRedThreads, 0, st>>>(partials, kRedBlocks, cplx ? 2 : 1, result);
+  return cudaGetLastError();
+}
+
+cudaError_t dot(const VS &v, const void *x, const void *y, double *partials, double *result, cudaStream_t st)
+{
+  if (v.ft != QB200_F16N) return dot(v.ft, v.n, x, y, partials, result, st);
+  return f16n_dot(v, false, x, y, partials, result, st);
+}
+
+cudaError_t cdot(const VS &v, const void *x, const void *y, double *partials, double *result, cudaStream_t st)
+{
+  if (v.ft != QB200_F16N) return cdot(v.ft, v.S, v.n, x, y, partials, result, st);
+  return f16n_dot(v, true, x, y, partials, result, st);
+}
+
+template <int S, bool TO>
+cudaError_t conv_f16n(int ft_plain, long long nsl, double scale, const void *in, void *out, cudaStream_t st)
+{
+  const int gr = grid_for(nsl);
+  switch (ft_plain) {
+  case QB200_F32: convert_f16n_kernel<S, float, TO><<<gr, 256, 0, st>>>(nsl, scale, in, out); break;
+  case QB200_F64: convert_f16n_kernel<S, double, TO><<<gr, 256, 0, st>>>(nsl, scale, in, out); break;
+  case QB200_BF16: convert_f16n_kernel<S, __nv_bfloat16, TO><<<gr, 256, 0, st>>>(nsl, scale, in, out); break;
+  default: convert_f16n_kernel<S, __half, TO><<<gr, 256, 0, st>>>(nsl, scale, in, out); break;
+  }
+  return cudaGetLastError();
+}
+
+// out = scale * in between two spinor arrays of the same lattice shape
+cudaError_t convert(const VS &vo, void *out, const VS &vi, const void *in, double scale, cudaStream_t st)
+{
+  if (vo.ft != QB200_F16N && vi.ft != QB200_F16N) return convert(vo.ft, out, vi.ft, in, vi.n, scale, st);
+  if (vo.ft == QB200_F16N && vi.ft == QB200_F16N) {
+    // copy, then rescale per site (decode, scale, re-encode)
+    cudaError_t e = cudaMemcpyAsync(out, in, vo.n * 2, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return e;
+    return axpby(vo, host(0.0), in, host(scale), out, st);
+  }
+  if (vo.ft == QB200_F16N) {
+    const long long nsl = vo.site_lanes();
+    QB_F16N_S(vo.S, return (conv_f16n<SS, true>(vi.ft, nsl, scale, in, out, st)));
+  } else {
+    const long long nsl = vi.site_lanes();
+    QB_F16N_S(vi.S, return (conv_f16n<SS, false>(vo.ft, nsl, scale, in, out, st)));
+  }
+  return cudaErrorInvalidValue;
 }
 
 // ---- the Schur operator ----------------------------------------------------
@@ -316,17 +428,16 @@ int normal_op(const qb200_lattice *l, const qb200_operator *op, const void *v, v
 int cg_core(const qb200_lattice *l, const qb200_operator *op, const void *rhs, void *x, double tol, int max_iter,
             const Vecs &s, int *iters, double *rel, cudaStream_t st)
 {
-  const int ft = l->ftype;
-  const long long n = spinor_elems(l);
+  const VS V = vs_of(l);
   void *r = s.v[0], *p = s.v[1], *Ap = s.v[2], *t = s.v[3], *tmp = s.v[4];
   double *rr_d = s.scal + 0, *rrn_d = s.scal + 1, *pAp_d = s.scal + 2, *bb_d = s.scal + 3;
   int rc;
   if ((rc = normal_op(l, op, x, Ap, t, tmp, st))) return rc;
   if ((rc = copy(r, rhs, spinor_bytes(l), st))) return rc;
-  cudaError_t e = axpby(ft, n, host(-1.0), Ap, host(1.0), r, st);
+  cudaError_t e = axpby(V, host(-1.0), Ap, host(1.0), r, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(p, r, spinor_bytes(l), cudaMemcpyDeviceToDevice, st);
-  if (e == cudaSuccess) e = dot(ft, n, r, r, s.partials, rr_d, st);
-  if (e == cudaSuccess) e = dot(ft, n, rhs, rhs, s.partials, bb_d, st);
+  if (e == cudaSuccess) e = dot(V, r, r, s.partials, rr_d, st);
+  if (e == cudaSuccess) e = dot(V, rhs, rhs, s.partials, bb_d, st);
   if ((rc = cuda_rc(e, "cg setup"))) return rc;
   double h[4];
   if ((rc = fetch(h, s.scal, 4, st))) return rc;
@@ -336,11 +447,11 @@ int cg_core(const qb200_lattice *l, const qb200_operator *op, const void *rhs, v
   int k = 0;
   while (rr > stop && k < max_iter) {
     if ((rc = normal_op(l, op, p, Ap, t, tmp, st))) return rc;
-    e = dot(ft, n, p, Ap, s.partials, pAp_d, st);
-    if (e == cudaSuccess) e = axpby(ft, n, ratio(rr_d, pAp_d, 1.0), p, host(1.0), x, st);
-    if (e == cudaSuccess) e = axpby(ft, n, ratio(rr_d, pAp_d, -1.0), Ap, host(1.0), r, st);
-    if (e == cudaSuccess) e = dot(ft, n, r, r, s.partials, rrn_d, st);
-    if (e == cudaSuccess) e = axpby(ft, n, host(1.0), r, ratio(rrn_d, rr_d, 1.0), p, st);
+    e = dot(V, p, Ap, s.partials, pAp_d, st);
+    if (e == cudaSuccess) e = axpby(V, ratio(rr_d, pAp_d, 1.0), p, host(1.0), x, st);
+    if (e == cudaSuccess) e = axpby(V, ratio(rr_d, pAp_d, -1.0), Ap, host(1.0), r, st);
+    if (e == cudaSuccess) e = dot(V, r, r, s.partials, rrn_d, st);
+    if (e == cudaSuccess) e = axpby(V, host(1.0), r, ratio(rrn_d, rr_d, 1.0), p, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(rr_d, rrn_d, sizeof(double), cudaMemcpyDeviceToDevice, st);
     if ((rc = cuda_rc(e, "cg iteration"))) return rc;
     if ((rc = fetch(&rr, rr_d, 1, st))) return rc;
@@ -357,19 +468,18 @@ int cg_core(const qb200_lattice *l, const qb200_operator *op, const void *rhs, v
 int bicgstab_core(const qb200_lattice *l, const qb200_operator *op, const void *b, void *x, double tol, int max_iter,
                   const Vecs &w, int *iters, double *rel, cudaStream_t st)
 {
-  const int ft = l->ftype, S = l->soalen;
-  const long long n = spinor_elems(l);
+  const VS V = vs_of(l);
   void *r = w.v[0], *r0 = w.v[1], *p = w.v[2], *v = w.v[3], *sv = w.v[4], *t = w.v[5], *tmp = w.v[6];
   double *d = w.scal;
   int rc;
   if ((rc = schur(l, op, 1, x, v, tmp, st))) return rc;
   if ((rc = copy(r, b, spinor_bytes(l), st))) return rc;
-  cudaError_t e = axpby(ft, n, host(-1.0), v, host(1.0), r, st);
+  cudaError_t e = axpby(V, host(-1.0), v, host(1.0), r, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(r0, r, spinor_bytes(l), cudaMemcpyDeviceToDevice, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(p, 0, spinor_bytes(l), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(v, 0, spinor_bytes(l), st);
-  if (e == cudaSuccess) e = dot(ft, n, b, b, w.partials, d + 0, st);
-  if (e == cudaSuccess) e = dot(ft, n, r, r, w.partials, d + 1, st);
+  if (e == cudaSuccess) e = dot(V, b, b, w.partials, d + 0, st);
+  if (e == cudaSuccess) e = dot(V, r, r, w.partials, d + 1, st);
   if ((rc = cuda_rc(e, "bicgstab setup"))) return rc;
   double h[2];
   if ((rc = fetch(h, d, 2, st))) return rc;
@@ -380,7 +490,7 @@ int bicgstab_core(const qb200_lattice *l, const qb200_operator *op, const void *
   int k = 0;
   while (rr > stop && k < max_iter) {
     // rho_new = <r0, r>
-    if ((e = cdot(ft, S, n, r0, r, w.partials, d + 2, st)) != cudaSuccess) return cuda_rc(e, "bicgstab");
+    if ((e = cdot(V, r0, r, w.partials, d + 2, st)) != cudaSuccess) return cuda_rc(e, "bicgstab");
     double c[2];
     if ((rc = fetch(c, d + 2, 2, st))) return rc;
     // beta = (rho_new / rho) (alpha / omega)
@@ -392,11 +502,11 @@ int bicgstab_core(const qb200_lattice *l, const qb200_operator *op, const void *
     rho_r = c[0];
     rho_i = c[1];
     // p = r + beta (p - omega v)
-    e = caxpby(ft, S, n, -om_r, -om_i, v, 1.0, 0.0, p, st);
-    if (e == cudaSuccess) e = caxpby(ft, S, n, 1.0, 0.0, r, be_r, be_i, p, st);
+    e = caxpby(V, -om_r, -om_i, v, 1.0, 0.0, p, st);
+    if (e == cudaSuccess) e = caxpby(V, 1.0, 0.0, r, be_r, be_i, p, st);
     if ((rc = cuda_rc(e, "bicgstab p"))) return rc;
     if ((rc = schur(l, op, 1, p, v, tmp, st))) return rc;
-    if ((e = cdot(ft, S, n, r0, v, w.partials, d + 4, st)) != cudaSuccess) return cuda_rc(e, "bicgstab");
+    if ((e = cdot(V, r0, v, w.partials, d + 4, st)) != cudaSuccess) return cuda_rc(e, "bicgstab");
     if ((rc = fetch(c, d + 4, 2, st))) return rc;
     const double dd = c[0] * c[0] + c[1] * c[1];
     if (dd == 0) return api_fail(QB200_EINVAL, "bicgstab breakdown");
@@ -404,11 +514,11 @@ int bicgstab_core(const qb200_lattice *l, const qb200_operator *op, const void *
     al_i = (rho_i * c[0] - rho_r * c[1]) / dd;
     // s = r - alpha v
     if ((rc = copy(sv, r, spinor_bytes(l), st))) return rc;
-    if ((e = caxpby(ft, S, n, -al_r, -al_i, v, 1.0, 0.0, sv, st)) != cudaSuccess) return cuda_rc(e, "bicgstab");
+    if ((e = caxpby(V, -al_r, -al_i, v, 1.0, 0.0, sv, st)) != cudaSuccess) return cuda_rc(e, "bicgstab");
     if ((rc = schur(l, op, 1, sv, t, tmp, st))) return rc;
     // omega = <t, s> / <t, t>
-    e = cdot(ft, S, n, t, sv, w.partials, d + 6, st);
-    if (e == cudaSuccess) e = dot(ft, n, t, t, w.partials, d + 8, st);
+    e = cdot(V, t, sv, w.partials, d + 6, st);
+    if (e == cudaSuccess) e = dot(V, t, t, w.partials, d + 8, st);
     if ((rc = cuda_rc(e, "bicgstab omega"))) return rc;
     double o[3];
     if ((rc = fetch(o, d + 6, 3, st))) return rc;
@@ -420,11 +530,11 @@ int bicgstab_core(const qb200_lattice *l, const qb200_operator *op, const void *
       om_i = o[1] / o[2];
     }
     // x += alpha p + omega s ; r = s - omega t
-    e = caxpby(ft, S, n, al_r, al_i, p, 1.0, 0.0, x, st);
-    if (e == cudaSuccess) e = caxpby(ft, S, n, om_r, om_i, sv, 1.0, 0.0, x, st);
+    e = caxpby(V, al_r, al_i, p, 1.0, 0.0, x, st);
+    if (e == cudaSuccess) e = caxpby(V, om_r, om_i, sv, 1.0, 0.0, x, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(r, sv, spinor_bytes(l), cudaMemcpyDeviceToDevice, st);
-    if (e == cudaSuccess) e = caxpby(ft, S, n, -om_r, -om_i, t, 1.0, 0.0, r, st);
-    if (e == cudaSuccess) e = dot(ft, n, r, r, w.partials, d + 1, st);
+    if (e == cudaSuccess) e = caxpby(V, -om_r, -om_i, t, 1.0, 0.0, r, st);
+    if (e == cudaSuccess) e = dot(V, r, r, w.partials, d + 1, st);
     if ((rc = cuda_rc(e, "bicgstab update"))) return rc;
     if ((rc = fetch(&rr, d + 1, 1, st))) return rc;
     k++;
@@ -439,12 +549,12 @@ int bicgstab_core(const qb200_lattice *l, const qb200_operator *op, const void *
 int true_residual(const qb200_lattice *l, const qb200_operator *op, const void *b, const void *x, void *r,
                   void *tmp, double *partials, double *scal, double *rel, cudaStream_t st)
 {
-  const long long n = spinor_elems(l);
+  const VS V = vs_of(l);
   int rc = schur(l, op, 1, x, r, tmp, st);
   if (rc) return rc;
-  cudaError_t e = axpby(l->ftype, n, host(1.0), b, host(-1.0), r, st);
-  if (e == cudaSuccess) e = dot(l->ftype, n, r, r, partials, scal, st);
-  if (e == cudaSuccess) e = dot(l->ftype, n, b, b, partials, scal + 1, st);
+  cudaError_t e = axpby(V, host(1.0), b, host(-1.0), r, st);
+  if (e == cudaSuccess) e = dot(V, r, r, partials, scal, st);
+  if (e == cudaSuccess) e = dot(V, b, b, partials, scal + 1, st);
   if ((rc = cuda_rc(e, "true residual"))) return rc;
   double h[2];
   if ((rc = fetch(h, scal, 2, st))) return rc;
@@ -466,7 +576,8 @@ long long qb200_blas_partials_len(void) { return kRedPartials; }
 
 int qb200_blas_axpby(int ftype, long long n, double a, const void *x, double b, void *y, void *stream)
 {
-  if (!ft_bytes(ftype)) return api_fail(QB200_ELAYOUT, "unknown storage type");
+  if (!ft_bytes(ftype) || ftype == QB200_F16N)
+    return api_fail(QB200_ELAYOUT, "unknown storage type (F16N spinors: use the lattice-aware solver entry points)");
   if (!x || !y) return api_fail(QB200_ENULL, "x and y must be non-NULL");
   if (n % 8) return api_fail(QB200_EINVAL, "n must be a multiple of 8");
   return cuda_rc(axpby(ftype, n, host(a), x, host(b), y, (cudaStream_t)stream), "axpby");
@@ -474,7 +585,8 @@ int qb200_blas_axpby(int ftype, long long n, double a, const void *x, double b, 
 
 int qb200_blas_convert(int ft_out, void *out, int ft_in, const void *in, long long n, double scale, void *stream)
 {
-  if (!ft_bytes(ft_out) || !ft_bytes(ft_in)) return api_fail(QB200_ELAYOUT, "unknown storage type");
+  if (!ft_bytes(ft_out) || !ft_bytes(ft_in) || ft_out == QB200_F16N || ft_in == QB200_F16N)
+    return api_fail(QB200_ELAYOUT, "unknown storage type (F16N spinors: use qb200_spinor_convert)");
   if (!in || !out) return api_fail(QB200_ENULL, "in and out must be non-NULL");
   return cuda_rc(convert(ft_out, out, ft_in, in, n, scale, (cudaStream_t)stream), "convert");
 }
@@ -482,7 +594,8 @@ int qb200_blas_convert(int ft_out, void *out, int ft_in, const void *in, long lo
 int qb200_blas_dot(int ftype, long long n, const void *x, const void *y, double *result, double *partials,
                    void *stream)
 {
-  if (!ft_bytes(ftype)) return api_fail(QB200_ELAYOUT, "unknown storage type");
+  if (!ft_bytes(ftype) || ftype == QB200_F16N)
+    return api_fail(QB200_ELAYOUT, "unknown storage type (F16N spinors: use the lattice-aware solver entry points)");
   if (!x || !y || !result || !partials) return api_fail(QB200_ENULL, "x, y, result and partials must be non-NULL");
   if (n % 8) return api_fail(QB200_EINVAL, "n must be a multiple of 8");
   return cuda_rc(dot(ftype, n, x, y, partials, result, (cudaStream_t)stream), "dot");
@@ -494,7 +607,17 @@ int qb200_blas_cdot(const qb200_lattice *lat, const void *x, const void *y, doub
   const long long n = qb200_spinor_elems(lat);
   if (n < 0) return api_fail(QB200_EINVAL, "invalid lattice");
   if (!x || !y || !result || !partials) return api_fail(QB200_ENULL, "x, y, result and partials must be non-NULL");
-  return cuda_rc(cdot(lat->ftype, lat->soalen, n, x, y, partials, result, (cudaStream_t)stream), "cdot");
+  return cuda_rc(cdot(vs_of(lat), x, y, partials, result, (cudaStream_t)stream), "cdot");
+}
+
+int qb200_spinor_convert(const qb200_lattice *lat_out, void *out, const qb200_lattice *lat_in, const void *in,
+                         double scale, void *stream)
+{
+  if (qb200_spinor_elems(lat_out) < 0 || qb200_spinor_elems(lat_in) < 0)
+    return api_fail(QB200_EINVAL, "invalid lattice");
+  if (!same_shape(lat_out, lat_in)) return api_fail(QB200_EINVAL, "lattices differ in shape");
+  if (!in || !out) return api_fail(QB200_ENULL, "in and out must be non-NULL");
+  return cuda_rc(convert(vs_of(lat_out), out, vs_of(lat_in), in, scale, (cudaStream_t)stream), "spinor convert");
 }
 
 int qb200_schur_apply(const qb200_lattice *lat, const qb200_operator *op, int isign, const void *in, void *out,
@@ -632,7 +755,8 @@ int qb200_invert_mixed(const qb200_lattice *lat_hi, const qb200_operator *op_hi,
   if (!b || !x || !ws_hi || !ws_lo) return api_fail(QB200_ENULL, "b, x and workspaces must be non-NULL");
   if (solver != 0 && solver != 1) return api_fail(QB200_EINVAL, "solver must be 0 (CG) or 1 (BiCGStab)");
   cudaStream_t st = (cudaStream_t)stream;
-  const long long n = spinor_elems(lat_hi);
+  const VS VH = vs_of(lat_hi), VL = vs_of(lat_lo);
+  const double ncomp = (double)VH.n; // components of one high-precision spinor array
   Vecs H = carve(lat_hi, ws_hi, 4);   // r, rn (normal residual), e, tmp
   Vecs L = carve(lat_lo, ws_lo, 9);   // solver vectors [0..6], rhs_lo [7], e_lo [8]
   void *r = H.v[0], *rn = H.v[1], *e_hi = H.v[2], *tmp = H.v[3];
@@ -641,7 +765,7 @@ int qb200_invert_mixed(const qb200_lattice *lat_hi, const qb200_operator *op_hi,
   if ((rc = cuda_rc(e, "mixed init"))) return rc;
   double bb;
   {
-    e = dot(lat_hi->ftype, n, b, b, H.partials, H.scal, st);
+    e = dot(VH, b, b, H.partials, H.scal, st);
     if ((rc = cuda_rc(e, "mixed |b|"))) return rc;
     if ((rc = fetch(&bb, H.scal, 1, st))) return rc;
   }
@@ -658,12 +782,12 @@ int qb200_invert_mixed(const qb200_lattice *lat_hi, const qb200_operator *op_hi,
       src = rn;
     }
     double rr;
-    e = dot(lat_hi->ftype, n, src, src, H.partials, H.scal + 4, st);
+    e = dot(VH, src, src, H.partials, H.scal + 4, st);
     if ((rc = cuda_rc(e, "mixed norm"))) return rc;
     if ((rc = fetch(&rr, H.scal + 4, 1, st))) return rc;
     // scale the low-precision right-hand side to O(1) components
-    const double scale = std::sqrt((double)n / (rr > 0 ? rr : 1.0));
-    e = convert(lat_lo->ftype, rhs_lo, lat_hi->ftype, src, n, scale, st);
+    const double scale = std::sqrt(ncomp / (rr > 0 ? rr : 1.0));
+    e = convert(VL, rhs_lo, VH, src, scale, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(e_lo, 0, spinor_bytes(lat_lo), st);
     if ((rc = cuda_rc(e, "mixed demote"))) return rc;
     int k = 0;
@@ -673,8 +797,8 @@ int qb200_invert_mixed(const qb200_lattice *lat_hi, const qb200_operator *op_hi,
     if (rc) return rc;
     tot += k;
     // x += e / scale (high precision)
-    e = convert(lat_hi->ftype, e_hi, lat_lo->ftype, e_lo, n, 1.0 / scale, st);
-    if (e == cudaSuccess) e = axpby(lat_hi->ftype, n, host(1.0), e_hi, host(1.0), x, st);
+    e = convert(VH, e_hi, VL, e_lo, 1.0 / scale, st);
+    if (e == cudaSuccess) e = axpby(VH, host(1.0), e_hi, host(1.0), x, st);
     if ((rc = cuda_rc(e, "mixed promote"))) return rc;
     outer++;
   }

@@ -84,7 +84,7 @@ class TSlabDslash:
         self.comm = comm
         self.k = kernels
         nface = g.face_sites(6)
-        self.bufs = [kernels.alloc(12 * nface) for _ in range(4)]  # send fwd, send back, recv back, recv fwd
+        self.bufs = [kernels.alloc(g.face_elems * nface) for _ in range(4)]  # send fwd, send back, recv back, recv fwd
 
     def apply(self, family, kernel, isign, cb, psi, out, gauge, chi=None, clover=None, coeff_s=1.0,
               coeff_t_f=1.0, coeff_t_b=1.0, alpha=1.0, mu=0.0, muinv=1.0, rho=0.0, tbc_mask=0,

@@ -16,10 +16,13 @@ from dataclasses import dataclass
 
 import torch
 
-F32, F64, F16 = 0, 1, 2
-FTYPE_NAMES = {F32: "f32", F64: "f64", F16: "f16"}
-TORCH_DTYPE = {F32: torch.float32, F64: torch.float64, F16: torch.float16}
-FT_BYTES = {F32: 4, F64: 8, F16: 2}
+F32, F64, F16, F16N, BF16 = 0, 1, 2, 3, 4
+FTYPE_NAMES = {F32: "f32", F64: "f64", F16: "f16", F16N: "f16n", BF16: "bf16"}
+# F16N: FP16 spinors with a per-site FP32 norm after each block; links and
+# clover plain FP16.  BF16: bfloat16 everywhere.
+TORCH_DTYPE = {F32: torch.float32, F64: torch.float64, F16: torch.float16, F16N: torch.float16,
+               BF16: torch.bfloat16}
+FT_BYTES = {F32: 4, F64: 8, F16: 2, F16N: 2, BF16: 2}
 
 
 class Lattice(ctypes.Structure):
@@ -108,8 +111,18 @@ class Geometry:
         return 2 if self.compress12 else 3
 
     @property
+    def spb(self):
+        """storage elements per lane of a spinor block"""
+        return 26 if self.ftype == F16N else 24
+
+    @property
+    def face_elems(self):
+        """storage elements per face site"""
+        return 14 if self.ftype == F16N else 12
+
+    @property
     def spinor_elems(self):
-        return self.nt * self.Pxyz * 24 * self.soalen
+        return self.nt * self.Pxyz * self.spb * self.soalen
 
     @property
     def gauge_elems(self):

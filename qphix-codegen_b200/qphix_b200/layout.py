@@ -16,7 +16,7 @@ off_diag[r(r-1)/2+c] holds element (r, c), r > c
 """
 import torch
 
-from .lattice import Geometry
+from .lattice import F16N, Geometry
 
 
 def cb_coords(g: Geometry, cb: int, device=None):
@@ -32,20 +32,39 @@ def cb_coords(g: Geometry, cb: int, device=None):
 
 
 def _blocks_to_flat(g: Geometry, blocks: torch.Tensor) -> torch.Tensor:
-    """blocks (nt, nz, ny, nvecs, 24*S) -> flat spinor field with padding."""
-    S = g.soalen
+    """blocks (nt, nz, ny, nvecs, B) -> flat spinor field with padding
+    (B = spb*S storage elements per block)."""
+    B = blocks.shape[-1]
     nt = g.nt
-    out = torch.zeros(nt, g.Pxyz * 24 * S, dtype=blocks.dtype, device=blocks.device)
-    body = out[:, : g.nz * g.Pxy * 24 * S].view(nt, g.nz, g.Pxy * 24 * S)
-    body[:, :, : g.ny * g.nvecs * 24 * S] = blocks.reshape(nt, g.nz, g.ny * g.nvecs * 24 * S)
+    out = torch.zeros(nt, g.Pxyz * B, dtype=blocks.dtype, device=blocks.device)
+    body = out[:, : g.nz * g.Pxy * B].view(nt, g.nz, g.Pxy * B)
+    body[:, :, : g.ny * g.nvecs * B] = blocks.reshape(nt, g.nz, g.ny * g.nvecs * B)
     return out.reshape(-1)
 
 
-def _flat_to_blocks(g: Geometry, flat: torch.Tensor) -> torch.Tensor:
+def _flat_to_blocks(g: Geometry, flat: torch.Tensor, B: int) -> torch.Tensor:
+    v = flat.reshape(g.nt, g.Pxyz * B)[:, : g.nz * g.Pxy * B]
+    v = v.reshape(g.nt, g.nz, g.Pxy * B)[:, :, : g.ny * g.nvecs * B]
+    return v.reshape(g.nt, g.nz, g.ny, g.nvecs, B)
+
+
+def _encode_f16n(g: Geometry, blocks: torch.Tensor) -> torch.Tensor:
+    """(..., 24*S) values -> (..., 26*S) halves: values / site norm, then the
+    FP32 norms of the S lanes as pairs of halves."""
     S = g.soalen
-    v = flat.reshape(g.nt, g.Pxyz * 24 * S)[:, : g.nz * g.Pxy * 24 * S]
-    v = v.reshape(g.nt, g.nz, g.Pxy * 24 * S)[:, :, : g.ny * g.nvecs * 24 * S]
-    return v.reshape(g.nt, g.nz, g.ny, g.nvecs, 24 * S)
+    v = blocks.reshape(*blocks.shape[:-1], 24, S)
+    nrm = v.abs().amax(dim=-2)                                   # (..., S)
+    nrm = torch.where(nrm > 0, nrm, torch.ones_like(nrm)).to(torch.float32)
+    h = (v / nrm.to(v.dtype).unsqueeze(-2)).to(torch.float16).reshape(*blocks.shape[:-1], 24 * S)
+    n16 = nrm.contiguous().view(torch.float16)                   # (..., 2*S)
+    return torch.cat([h, n16], dim=-1)
+
+
+def _decode_f16n(g: Geometry, blocks: torch.Tensor) -> torch.Tensor:
+    S = g.soalen
+    h = blocks[..., : 24 * S].to(torch.float64).reshape(*blocks.shape[:-1], 24, S)
+    nrm = blocks[..., 24 * S:].contiguous().view(torch.float32).to(torch.float64)
+    return (h * nrm.unsqueeze(-2)).reshape(*blocks.shape[:-1], 24 * S)
 
 
 def pack_spinor(g: Geometry, sp: torch.Tensor, dtype=None) -> torch.Tensor:
@@ -55,13 +74,19 @@ def pack_spinor(g: Geometry, sp: torch.Tensor, dtype=None) -> torch.Tensor:
     r = torch.view_as_real(sp.to(torch.complex128).resolve_conj())        # nt nz ny nxh 4 3 2
     r = r.reshape(g.nt, g.nz, g.ny, g.nvecs, S, 4, 3, 2)
     r = r.permute(0, 1, 2, 3, 6, 5, 7, 4)                    # .. nvecs c s ri S
-    return _blocks_to_flat(g, r.reshape(g.nt, g.nz, g.ny, g.nvecs, 24 * S).to(dtype))
+    r = r.reshape(g.nt, g.nz, g.ny, g.nvecs, 24 * S)
+    if g.ftype == F16N and dtype == torch.float16:
+        return _blocks_to_flat(g, _encode_f16n(g, r))
+    return _blocks_to_flat(g, r.to(dtype))
 
 
 def unpack_spinor(g: Geometry, flat: torch.Tensor) -> torch.Tensor:
     """FourSpinorBlock array -> canonical complex128 checkerboard spinor."""
     S = g.soalen
-    b = _flat_to_blocks(g, flat.to(torch.float64))
+    if g.ftype == F16N and flat.dtype == torch.float16:
+        b = _decode_f16n(g, _flat_to_blocks(g, flat, 26 * S))
+    else:
+        b = _flat_to_blocks(g, flat.to(torch.float64), 24 * S)
     b = b.reshape(g.nt, g.nz, g.ny, g.nvecs, 3, 4, 2, S).permute(0, 1, 2, 3, 7, 5, 4, 6)
     b = b.reshape(g.nt, g.nz, g.ny, g.nxh, 4, 3, 2).contiguous()
     return torch.view_as_complex(b)

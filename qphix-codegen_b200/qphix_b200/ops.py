@@ -91,7 +91,7 @@ def face_pack(g: Geometry, isign, psi_cb, psi, outbuf, dir, stream=None):
     L = _lib.lib()
     fn = L.qb200_face_proj_dir_plus if isign > 0 else L.qb200_face_proj_dir_minus
     _check_field("psi", psi, g, g.spinor_elems)
-    _check_field("outbuf", outbuf, g, g.face_sites(dir) * 12)
+    _check_field("outbuf", outbuf, g, g.face_sites(dir) * g.face_elems)
     lat = g.c_struct()
     _lib.check(fn(ctypes.byref(lat), psi_cb, _ptr(psi), _ptr(outbuf), dir, _stream(stream)))
     return outbuf
@@ -102,7 +102,7 @@ def face_unpack(g: Geometry, family, isign, cb, inbuf, gauge, out, dir, *, beta=
     """face_*finish_dir: accumulate the face contribution of dir into out."""
     L = _lib.lib()
     pm = "plus" if isign > 0 else "minus"
-    _check_field("inbuf", inbuf, g, g.face_sites(dir) * 12)
+    _check_field("inbuf", inbuf, g, g.face_sites(dir) * g.face_elems)
     _check_field("gauge", gauge, g, g.gauge_elems)
     _check_field("out", out, g, g.spinor_elems)
     lat = g.c_struct()

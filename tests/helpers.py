@@ -12,9 +12,28 @@ for p in (REPO, PKG):
         sys.path.insert(0, p)
 
 from qphix_b200 import fields, layout  # noqa: E402
-from qphix_b200.lattice import F16, F32, F64, Geometry  # noqa: E402
+from qphix_b200.lattice import BF16, F16, F16N, F32, F64, Geometry  # noqa: E402
 
-NP_DTYPE = {F32: np.float32, F64: np.float64, F16: np.float16}
+# numpy carries bfloat16 arrays as their uint16 bit patterns
+NP_DTYPE = {F32: np.float32, F64: np.float64, F16: np.float16, F16N: np.float16, BF16: np.uint16}
+
+
+def to_np(t):
+    """storage tensor -> numpy array (bfloat16 as uint16 bits)"""
+    t = t.detach().cpu().contiguous()
+    if t.dtype == torch.bfloat16:
+        return t.view(torch.int16).numpy().view(np.uint16)
+    return t.numpy()
+
+
+def to_torch(a, device=None):
+    """numpy storage array -> torch tensor (uint16 bits -> bfloat16)"""
+    a = np.ascontiguousarray(a)
+    if a.dtype == np.uint16:
+        t = torch.from_numpy(a.view(np.int16)).view(torch.bfloat16)
+    else:
+        t = torch.from_numpy(a)
+    return t.to(device) if device is not None else t
 FAMILIES = ("wilson", "clover", "tm", "tm_clover")
 KERNELS = ("dslash", "achimbdpsi")
 
@@ -29,14 +48,13 @@ def make_fields(g: Geometry, seed=1234, cb=0, inverse_clover=False):
     if inverse_clover:
         A = fields.invert_blocks(A)
     F = fields.random_full_clover(g, seed=seed + 4)
-    dt = NP_DTYPE[g.ftype]
     out = {
         "U": U,
-        "psi": layout.pack_spinor(g, psi, torch.float64).numpy().astype(dt),
-        "chi": layout.pack_spinor(g, chi, torch.float64).numpy().astype(dt),
-        "gauge": layout.pack_gauge(g, U, cb, torch.float64).numpy().astype(dt),
-        "clover": layout.pack_clover(g, A, torch.float64).numpy().astype(dt),
-        "fclover": layout.pack_full_clover(g, F, torch.float64).numpy().astype(dt),
+        "psi": to_np(layout.pack_spinor(g, psi)),
+        "chi": to_np(layout.pack_spinor(g, chi)),
+        "gauge": to_np(layout.pack_gauge(g, U, cb)),
+        "clover": to_np(layout.pack_clover(g, A)),
+        "fclover": to_np(layout.pack_full_clover(g, F)),
     }
     return out
 
@@ -44,10 +62,8 @@ def make_fields(g: Geometry, seed=1234, cb=0, inverse_clover=False):
 def site_rel_err(g: Geometry, a, b):
     """max over components of |a-b| / max(|b_i|, |b_site|/sqrt(24)) -- the
     per-component relative error with a floor at the site's rms component."""
-    a = np.asarray(a, dtype=np.float64)[: g.spinor_elems]
-    b = np.asarray(b, dtype=np.float64)[: g.spinor_elems]
-    ta = layout.unpack_spinor(g, torch.from_numpy(a)).numpy().reshape(-1, 12)
-    tb = layout.unpack_spinor(g, torch.from_numpy(b)).numpy().reshape(-1, 12)
+    ta = layout.unpack_spinor(g, to_torch(np.asarray(a)[: g.spinor_elems])).numpy().reshape(-1, 12)
+    tb = layout.unpack_spinor(g, to_torch(np.asarray(b)[: g.spinor_elems])).numpy().reshape(-1, 12)
     ra = np.concatenate([ta.real, ta.imag], axis=1)
     rb = np.concatenate([tb.real, tb.imag], axis=1)
     site = np.sqrt((rb ** 2).sum(axis=1, keepdims=True) / 24.0)

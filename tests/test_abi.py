@@ -8,7 +8,7 @@ import re
 import pytest
 
 from qphix_b200 import _lib
-from qphix_b200.lattice import F32, Geometry
+from qphix_b200.lattice import BF16, F16N, F32, Geometry
 
 HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "qphix_b200.h")
 
@@ -41,7 +41,8 @@ def test_library_exports_every_declared_symbol():
 def test_sizes_match_python_geometry():
     L = _lib.lib()
     for g in (Geometry(8, 8, 4, 4, soalen=4, veclen=8), Geometry(32, 4, 4, 2, soalen=16, compress12=True),
-              Geometry(4, 4, 4, 6, soalen=1, pad_xy=3, pad_xyz=1)):
+              Geometry(4, 4, 4, 6, soalen=1, pad_xy=3, pad_xyz=1),
+              Geometry(16, 8, 4, 4, soalen=8, ftype=F16N, pad_xy=1), Geometry(8, 8, 4, 4, soalen=4, ftype=BF16)):
         lat = g.c_struct()
         assert L.qb200_spinor_elems(ctypes.byref(lat)) == g.spinor_elems
         assert L.qb200_gauge_elems(ctypes.byref(lat)) == g.gauge_elems
@@ -70,6 +71,9 @@ def test_argument_errors_are_status_codes():
     assert _call_plus(bad) == -3
     bad = g.c_struct()
     bad.ftype = 9
+    assert _call_plus(bad) == -3
+    assert L.qb200_layout_supported(3, 2) == 0 and L.qb200_layout_supported(3, 8) == 1
+    bad = Geometry(8, 8, 4, 4, soalen=2, ftype=F16N).c_struct()
     assert _call_plus(bad) == -3
     assert _call_plus(g.c_struct(), cb=2) == -1
     assert _call_plus(g.c_struct(), psi=0) == -2

@@ -9,21 +9,23 @@ import torch
 import helpers as H
 import oracle as O
 from qphix_b200 import ops
-from qphix_b200.lattice import F16, F32, F64, Geometry
+from qphix_b200.lattice import BF16, F16, F16N, F32, F64, Geometry
 
-TOL = {F32: 2e-6, F64: 1e-13, F16: 1e-3}
+# FP16 with a per-site norm quantises every component to 2^-11 of the site's
+# largest one, bfloat16 to 2^-8 of each value
+TOL = {F32: 2e-6, F64: 1e-13, F16: 1e-3, F16N: 2e-3, BF16: 1e-2}
 
 pytestmark = pytest.mark.gpu
 
 
 def _run_gpu(g, f, fam, kernel, isign, cb, pp, dev):
-    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    T = lambda a: H.to_torch(a, dev)
     psi, chi, gauge = T(f["psi"]), T(f["chi"]), T(f["gauge"])
     cl = T(f["fclover"] if fam == "tm_clover" else f["clover"])
     out = torch.zeros_like(psi)
     ops.dslash(g, fam, kernel, isign, cb, psi, out, gauge, chi=chi, clover=cl, **pp)
     torch.cuda.synchronize()
-    return out.cpu().numpy()
+    return H.to_np(out)
 
 
 def _run_oracle(g, f, fam, kernel, isign, cb, pp):
@@ -35,6 +37,7 @@ def _run_oracle(g, f, fam, kernel, isign, cb, pp):
 LAYOUTS = [
     (1, 1, F32), (2, 2, F32), (4, 4, F32), (4, 16, F32), (8, 8, F32), (16, 16, F32),
     (4, 8, F64), (8, 8, F64), (4, 16, F16), (8, 8, F16), (16, 16, F16),
+    (4, 8, F16N), (16, 16, F16N), (8, 16, BF16), (16, 16, BF16),
 ]
 
 

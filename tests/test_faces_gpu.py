@@ -9,26 +9,34 @@ import helpers as H
 import oracle as O
 from qphix_b200 import fields, layout, ops
 from qphix_b200.halo import GPUKernels, face_kind, local_geometry
-from qphix_b200.lattice import F16, F32, F64, Geometry
+from qphix_b200.lattice import BF16, F16, F16N, F32, F64, Geometry
 
 pytestmark = pytest.mark.gpu
-TOL = {F32: 2e-6, F64: 1e-13, F16: 1e-3}
-LAYOUTS = [(1, 1, F32), (4, 16, F32), (16, 16, F32), (2, 4, F64), (8, 8, F16)]
+TOL = {F32: 2e-6, F64: 1e-13, F16: 1e-3, F16N: 2e-3, BF16: 1e-2}
+LAYOUTS = [(1, 1, F32), (4, 16, F32), (16, 16, F32), (2, 4, F64), (8, 8, F16), (8, 8, F16N), (4, 16, BF16)]
+
+
+def _face_values(g, buf):
+    """decoded face values (n, 12) as float64"""
+    b = buf.detach().cpu()
+    if g.ftype == F16N:
+        r = b.reshape(-1, 14)
+        return (r[:, :12].double() * r[:, 12:].contiguous().view(torch.float32).double()).numpy()
+    return b.double().reshape(-1, 12).numpy()
 
 
 @pytest.mark.parametrize("soa,vec,ft", LAYOUTS)
 def test_face_pack(cuda, soa, vec, ft):
     g = Geometry(max(4, 2 * soa), 8, 4, 6, soalen=soa, veclen=vec, ftype=ft)
     f = H.make_fields(g, cb=0, seed=31)
-    psi = torch.from_numpy(f["psi"]).to(cuda)
+    psi = H.to_torch(f["psi"], cuda)
     for d in range(8):
         for isign in (1, -1):
-            buf = torch.zeros(12 * g.face_sites(d), dtype=g.dtype, device=cuda)
+            buf = torch.zeros(g.face_elems * g.face_sites(d), dtype=g.dtype, device=cuda)
             ops.face_pack(g, isign, 1, psi, buf, d)
             ref = O.face_pack(g, isign, 1, f["psi"], d)
-            a = buf.cpu().numpy().astype(np.float64)
-            scale = np.abs(ref).max()
-            assert np.abs(a - ref).max() <= TOL[ft] * scale * 4, (d, isign)
+            a, r = _face_values(g, buf), _face_values(g, H.to_torch(ref))
+            assert np.abs(a - r).max() <= TOL[ft] * np.abs(r).max() * 4, (d, isign)
 
 
 @pytest.mark.parametrize("soa,vec,ft", LAYOUTS)
@@ -38,21 +46,24 @@ def test_face_unpack(cuda, soa, vec, ft):
     rng = np.random.default_rng(5)
     for fam in H.FAMILIES:
         cl_np = f["fclover" if fam == "tm_clover" else "clover"]
-        cl = torch.from_numpy(cl_np).to(cuda)
-        gauge = torch.from_numpy(f["gauge"]).to(cuda)
+        cl = H.to_torch(cl_np, cuda)
+        gauge = H.to_torch(f["gauge"], cuda)
         for d in range(8):
             for isign in (1, -1):
                 n = g.face_sites(d)
-                inbuf_np = rng.normal(size=12 * n).astype(f["psi"].dtype)
+                # a face buffer in the storage format: pack a random spinor's face
+                src = H.make_fields(g, cb=1, seed=40 + d)["psi"]
+                inbuf_np = O.face_pack(g, isign, 1, src, d ^ 1)
                 pp = H.op_params(fam, "dslash")
                 tbc = (d + isign) % 3 == 0
-                out = torch.from_numpy(f["chi"]).to(cuda)
-                ops.face_unpack(g, fam, isign, 0, torch.from_numpy(inbuf_np).to(cuda), gauge, out, d, beta=0.41,
+                out = H.to_torch(f["chi"], cuda)
+                ops.face_unpack(g, fam, isign, 0, H.to_torch(inbuf_np, cuda), gauge, out, d, beta=0.41,
                                 clover=cl, mu=pp["mu"], muinv=pp["muinv"], tbc=tbc, tbc_phases=pp["tbc_phases"])
                 ref = O.face_unpack(g, fam, isign, 0, inbuf_np, f["gauge"], f["chi"].copy(), d, beta=0.41,
                                     clover=cl_np, mu=pp["mu"], muinv=pp["muinv"], tbc=tbc,
                                     tbc_phases=pp["tbc_phases"])
-                e = H.site_rel_err(g, out.cpu().numpy(), ref)
+                assert n * g.face_elems == inbuf_np.size
+                e = H.site_rel_err(g, H.to_np(out), ref)
                 assert e < TOL[ft], (fam, d, isign, e)
 
 

@@ -7,7 +7,7 @@ import torch
 
 import helpers as H
 from qphix_b200 import _lib, layout
-from qphix_b200.lattice import F16, F32, F64, Geometry
+from qphix_b200.lattice import BF16, F16, F16N, F32, F64, Geometry
 from qphix_b200.solver import EvenOddOperator, mixed_solve
 
 pytestmark = pytest.mark.gpu
@@ -95,7 +95,7 @@ def test_cg_and_bicgstab_fp64(cuda, family):
     assert _true_res(g, family, f, p, x2.cpu().numpy()) < 1e-10
 
 
-@pytest.mark.parametrize("lo", [F32, F16])
+@pytest.mark.parametrize("lo", [F32, F16, F16N, BF16])
 @pytest.mark.parametrize("solver", ["cg", "bicgstab"])
 def test_mixed_precision_reaches_1e10(cuda, lo, solver):
     family = "clover"
@@ -103,9 +103,9 @@ def test_mixed_precision_reaches_1e10(cuda, lo, solver):
     f, p = H.eo_setup(g, family)
     op64 = _op(g, family, f, p, cuda)
     glo = g.with_(ftype=lo)
-    oplo = _op(glo, family, f, p, cuda, dtype=glo.dtype)
+    oplo = _op(glo, family, f, p, cuda, dtype=glo.dtype)   # links / clover in the low type
     b = torch.from_numpy(f["b"]).to(cuda)
-    x, info = mixed_solve(op64, oplo, b, solver=solver, tol=1e-10, inner_tol=1e-2 if lo == F16 else 1e-4)
+    x, info = mixed_solve(op64, oplo, b, solver=solver, tol=1e-10, inner_tol=1e-4 if lo == F32 else 1e-2)
     assert info["rel_res"] <= 1e-10, info
     assert _true_res(g, family, f, p, x.cpu().numpy()) < 2e-10
     print(solver, lo, info)
