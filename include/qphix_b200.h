@@ -412,6 +412,51 @@ int qb200_invert_mixed(const qb200_lattice *lat_hi, const qb200_operator *op_hi,
                        double inner_tol, int max_inner, int max_outer, void *ws_hi, void *ws_lo,
                        int *inner_iters, int *outer_iters, double *rel_res, void *stream);
 
+/*
+ * ---- multi-right-hand-side operator -------------------------------------
+ * No counterpart in the reference.  A multi-RHS spinor array holds nrhs
+ * (1, 2, 4, 8 or 16) fields of one checkerboard with the right-hand side innermost:
+ * FT[block][3 colour][4 spin][2 re/im][S][nrhs] (blocks and padding as in the
+ * single layout).  Links and clover are shared by all right-hand sides, so
+ * their bytes are read once per nrhs solutions.  Built for FP32 and FP16
+ * storage, soalen 4, 8, 16.
+ */
+typedef struct qb200_coeffs {
+  double coeff_s, coeff_t_f, coeff_t_b;
+  double alpha, mu, muinv, rho;
+  unsigned tbc_mask;
+  double tbc_phases[4][2];
+} qb200_coeffs;
+
+long long qb200_mrhs_spinor_elems(const qb200_lattice *lat, int nrhs);
+/* gather nrhs single-layout fields (host array of device pointers) into one
+ * multi-RHS array, and scatter back */
+int qb200_mrhs_pack(const qb200_lattice *lat, int nrhs, const void *const *fields, void *mrhs, void *stream);
+int qb200_mrhs_unpack(const qb200_lattice *lat, int nrhs, const void *mrhs, void *const *fields, void *stream);
+/* the body kernels on multi-RHS arrays: family 0..3 (wilson, clover, tm,
+ * tm_clover), achimbdpsi 0/1, isign +1/-1; the meaning of every scalar is
+ * that of the single-RHS entry points */
+int qb200_dslash_mrhs(const qb200_lattice *lat, int nrhs, int family, int achimbdpsi, int isign, int cb,
+                      const void *psi, const void *chi, void *out, const void *gauge, const void *clover,
+                      const qb200_coeffs *coeffs, const unsigned accumulate[8], void *stream);
+int qb200_schur_apply_mrhs(const qb200_lattice *lat, int nrhs, const qb200_operator *op, int isign, const void *in,
+                           void *out, void *tmp_other_cb, void *stream);
+/* CG on the normal equations for nrhs systems sharing operator applications;
+ * rel_res[nrhs] receives |r|/|rhs| of each normal-equation residual */
+long long qb200_cg_mrhs_workspace_bytes(const qb200_lattice *lat, int nrhs);
+int qb200_invert_cg_mrhs(const qb200_lattice *lat, int nrhs, const qb200_operator *op, const void *b, void *x,
+                         double rel_tol, int max_iter, void *workspace, int *iters, double *rel_res, void *stream);
+/* nrhs systems Mhat x_i = b_i in FP64 (b, x: host arrays of nrhs device
+ * pointers to FP64 single-layout spinors, lat_hi FP64) with the corrections
+ * solved together by the multi-RHS low-precision operator (lat_lo FP16 or
+ * FP32); rel_res[nrhs] = |b_i - Mhat x_i| / |b_i| */
+long long qb200_mixed_mrhs_workspace_bytes(const qb200_lattice *lat_hi, const qb200_lattice *lat_lo, int nrhs,
+                                           long long *lo_bytes);
+int qb200_invert_mixed_mrhs(const qb200_lattice *lat_hi, const qb200_operator *op_hi, const qb200_lattice *lat_lo,
+                            const qb200_operator *op_lo, int nrhs, const void *const *b, void *const *x,
+                            double rel_tol, double inner_tol, int max_inner, int max_outer, void *ws_hi, void *ws_lo,
+                            int *inner_iters, int *outer_iters, double *rel_res, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

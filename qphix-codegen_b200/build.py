@@ -26,6 +26,7 @@ NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
 FTYPES = {"f32": "float", "f64": "double", "f16": "__half", "f16n": "half_norm", "bf16": "__nv_bfloat16"}
 SOALENS = [1, 2, 4, 8, 16]
 WIDE_ONLY = ("f16n", "bf16")   # built for SOALEN 4, 8, 16
+MRHS = ("f32", "f16")           # multi-RHS kernels, SOALEN 4, 8, 16
 
 
 def nvcc():
@@ -38,13 +39,15 @@ def nvcc():
 def units():
     """(object path, extra flags, source) for every translation unit."""
     out = [(os.path.join(BUILD, "qb200_api.o"), [], os.path.join(CSRC, "qb200_api.cu")),
-           (os.path.join(BUILD, "qb200_solver.o"), [], os.path.join(CSRC, "qb200_solver.cu"))]
+           (os.path.join(BUILD, "qb200_solver.o"), [], os.path.join(CSRC, "qb200_solver.cu")),
+           (os.path.join(BUILD, "qb200_mrhs.o"), [], os.path.join(CSRC, "qb200_mrhs.cu"))]
     for tag, ft in FTYPES.items():
         for s in SOALENS:
             if tag in WIDE_ONLY and s < 4:
                 continue
+            mr = 1 if (tag in MRHS and s >= 4) else 0
             out.append((os.path.join(BUILD, "inst_%s_s%d.o" % (tag, s)),
-                        ["-DQB_FT=%s" % ft, "-DQB_S=%d" % s],
+                        ["-DQB_FT=%s" % ft, "-DQB_S=%d" % s, "-DQB_MRHS=%d" % mr],
                         os.path.join(CSRC, "qb200_inst.cu")))
     return out
 

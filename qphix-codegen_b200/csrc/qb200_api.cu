@@ -71,6 +71,7 @@ int make_geo(const qb200_lattice *l, GeoDev &g)
   g.Pxy = (long long)l->ny * g.nvecs + l->pad_xy;
   g.Pxyz = (long long)l->nz * g.Pxy + l->pad_xyz;
   g.nsites = (int)nsites;
+  g.nrhs = 1;
   return QB200_OK;
 }
 
@@ -312,8 +313,15 @@ long long elem_count(const qb200_lattice *l, int what)
 } // namespace
 
 namespace qb200 {
-// shared with the solver translation unit
+// shared with the solver translation units
 int api_fail(int code, const char *msg) { return fail(code, "%s", msg); }
+int api_geo(const qb200_lattice *l, GeoDev &g) { return make_geo(l, g); }
+int api_check_device() { return check_device(); }
+void api_fill_op_f(OpDev<float> &p, const qb200_lattice *l, int isPlus, int cb, bool negate, double cs, double ctf,
+                   double ctb, unsigned tbc_mask, const double *ph, const unsigned *acc)
+{
+  fill_op<float>(p, l, isPlus, cb, negate, cs, ctf, ctb, tbc_mask, ph, acc);
+}
 
 int api_body(const qb200_lattice *l, int fam, bool ach, int isPlus, int cb, const void *psi, const void *chi,
              const void *gauge, const void *clov, void *out, const unsigned *accumulate, double coeff_s,

@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(256) convert_kernel(long long n, double scale,
 // ---------------------------------------------------------------------------
 // reductions
 
-__device__ __forceinline__ double warp_sum(double v)
+static __device__ __forceinline__ double warp_sum(double v)
 {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -123,7 +123,7 @@ __device__ __forceinline__ double warp_sum(double v)
 }
 
 // block sum of two values; thread 0 holds the result
-__device__ __forceinline__ void block_sum2(double &a, double &b)
+static __device__ __forceinline__ void block_sum2(double &a, double &b)
 {
   __shared__ double sa[32], sb[32];
   a = warp_sum(a);
@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(kRedThreads) cdot_partial_kernel(long long npa
 }
 
 // result[c] = sum of partials[c*kRedBlocks .. +nblocks) for c < ncomp
-__global__ void __launch_bounds__(kRedThreads) finish_kernel(const double *__restrict__ partials, int nblocks,
+static __global__ void __launch_bounds__(kRedThreads) finish_kernel(const double *__restrict__ partials, int nblocks,
                                                              int ncomp, double *__restrict__ result)
 {
   double a = 0.0, b = 0.0;

@@ -100,6 +100,7 @@ struct GeoDev {
   int nxh, nvecs, ngy, nyg, V;
   long long Pxy, Pxyz;
   int nsites; // nxh*ny*nz*nt
+  int nrhs;   // right-hand sides interleaved innermost (multi-RHS layout), else 1
 };
 
 // run-time operator parameters, arithmetic type C
@@ -255,6 +256,41 @@ __device__ __forceinline__ void store_spinor(elem_t<FT> *__restrict__ f, long lo
     for (int s = 0; s < 4; s++) {
       ftraits<FT>::st(f + base + ((c * 4 + s) * 2 + 0) * S, sp[s][c].re * scale);
       ftraits<FT>::st(f + base + ((c * 4 + s) * 2 + 1) * S, sp[s][c].im * scale);
+    }
+}
+
+// multi-RHS layout: block = FT[3][4][2][S][nrhs] (no per-site norms);
+// component k of lane l, right-hand side r at blk*24*S*nrhs + k*S*nrhs + l*nrhs + r
+template <int S>
+__device__ __forceinline__ long long spinor_base_mr(const GeoDev &g, const Site &s, int r)
+{
+  long long blk = s.t * g.Pxyz + s.z * g.Pxy + (long long)s.y * g.nvecs + s.xcb / S;
+  return (blk * (24 * S) + (s.xcb % S)) * g.nrhs + r;
+}
+
+template <typename FT>
+__device__ __forceinline__ void load_spinor_rs(const elem_t<FT> *__restrict__ f, long long base, int cs,
+                                               cx<comp_t<FT>> (&sp)[4][3])
+{
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      sp[s][c].re = ftraits<FT>::ld(f + base + (long long)((c * 4 + s) * 2 + 0) * cs);
+      sp[s][c].im = ftraits<FT>::ld(f + base + (long long)((c * 4 + s) * 2 + 1) * cs);
+    }
+}
+
+template <typename FT>
+__device__ __forceinline__ void store_spinor_rs(elem_t<FT> *__restrict__ f, long long base, int cs,
+                                                const cx<comp_t<FT>> (&sp)[4][3])
+{
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      ftraits<FT>::st(f + base + (long long)((c * 4 + s) * 2 + 0) * cs, sp[s][c].re);
+      ftraits<FT>::st(f + base + (long long)((c * 4 + s) * 2 + 1) * cs, sp[s][c].im);
     }
 }
 

@@ -16,28 +16,29 @@ namespace qb200 {
 namespace {
 constexpr int kThreads = 128;
 
-template <typename FT, int S, bool COMP12, int FAM, bool ACH>
+template <typename FT, int S, bool COMP12, int FAM, bool ACH, bool MR>
 cudaError_t go(const KArgs<FT> &a, const GeoDev &g, const OpDev<typename ftraits<FT>::C> &p,
                cudaStream_t st)
 {
-  const int blocks = (g.nsites + kThreads - 1) / kThreads;
-  site_dslash_kernel<FT, S, COMP12, FAM, ACH><<<blocks, kThreads, 0, st>>>(a, g, p);
+  const long long n = (long long)g.nsites * (MR ? g.nrhs : 1);
+  const int blocks = (int)((n + kThreads - 1) / kThreads);
+  site_dslash_kernel<FT, S, COMP12, FAM, ACH, MR><<<blocks, kThreads, 0, st>>>(a, g, p);
   return cudaGetLastError();
 }
 
-template <typename FT, int S, bool COMP12>
+template <typename FT, int S, bool COMP12, bool MR>
 cudaError_t go_fam(const LaunchSpec &ls, const KArgs<FT> &a, const GeoDev &g,
                    const OpDev<typename ftraits<FT>::C> &p, cudaStream_t st)
 {
   switch (ls.fam * 2 + (ls.ach ? 1 : 0)) {
-  case 0: return go<FT, S, COMP12, FAM_WILSON, false>(a, g, p, st);
-  case 1: return go<FT, S, COMP12, FAM_WILSON, true>(a, g, p, st);
-  case 2: return go<FT, S, COMP12, FAM_CLOVER, false>(a, g, p, st);
-  case 3: return go<FT, S, COMP12, FAM_CLOVER, true>(a, g, p, st);
-  case 4: return go<FT, S, COMP12, FAM_TM, false>(a, g, p, st);
-  case 5: return go<FT, S, COMP12, FAM_TM, true>(a, g, p, st);
-  case 6: return go<FT, S, COMP12, FAM_TMCLOV, false>(a, g, p, st);
-  case 7: return go<FT, S, COMP12, FAM_TMCLOV, true>(a, g, p, st);
+  case 0: return go<FT, S, COMP12, FAM_WILSON, false, MR>(a, g, p, st);
+  case 1: return go<FT, S, COMP12, FAM_WILSON, true, MR>(a, g, p, st);
+  case 2: return go<FT, S, COMP12, FAM_CLOVER, false, MR>(a, g, p, st);
+  case 3: return go<FT, S, COMP12, FAM_CLOVER, true, MR>(a, g, p, st);
+  case 4: return go<FT, S, COMP12, FAM_TM, false, MR>(a, g, p, st);
+  case 5: return go<FT, S, COMP12, FAM_TM, true, MR>(a, g, p, st);
+  case 6: return go<FT, S, COMP12, FAM_TMCLOV, false, MR>(a, g, p, st);
+  case 7: return go<FT, S, COMP12, FAM_TMCLOV, true, MR>(a, g, p, st);
   }
   return cudaErrorInvalidValue;
 }
@@ -76,8 +77,25 @@ cudaError_t launch_dslash(const LaunchSpec &ls, const elem_t<FT> *psi, const ele
   a.clov = clov;
   a.out = out;
   if (g.nsites == 0) return cudaSuccess;
-  return ls.comp12 ? go_fam<FT, S, true>(ls, a, g, p, st) : go_fam<FT, S, false>(ls, a, g, p, st);
+  return ls.comp12 ? go_fam<FT, S, true, false>(ls, a, g, p, st) : go_fam<FT, S, false, false>(ls, a, g, p, st);
 }
+
+#if QB_MRHS
+template <typename FT, int S>
+cudaError_t launch_dslash_mrhs(const LaunchSpec &ls, const elem_t<FT> *psi, const elem_t<FT> *chi,
+                               const elem_t<FT> *gauge, const elem_t<FT> *clov, elem_t<FT> *out, const GeoDev &g,
+                               const OpDev<comp_t<FT>> &p, cudaStream_t st)
+{
+  KArgs<FT> a;
+  a.psi = psi;
+  a.chi = chi;
+  a.gauge = gauge;
+  a.clov = clov;
+  a.out = out;
+  if (g.nsites == 0) return cudaSuccess;
+  return ls.comp12 ? go_fam<FT, S, true, true>(ls, a, g, p, st) : go_fam<FT, S, false, true>(ls, a, g, p, st);
+}
+#endif
 
 template <typename FT, int S>
 cudaError_t launch_face_pack(const elem_t<FT> *psi, elem_t<FT> *buf, const GeoDev &g, const FaceSpec &fs,
@@ -116,6 +134,11 @@ template cudaError_t launch_dslash<QB_FT, QB_S>(const LaunchSpec &, const QB_E *
                                                 cudaStream_t);
 template cudaError_t launch_face_pack<QB_FT, QB_S>(const QB_E *, QB_E *, const GeoDev &, const FaceSpec &, int,
                                                    cudaStream_t);
+#if QB_MRHS
+template cudaError_t launch_dslash_mrhs<QB_FT, QB_S>(const LaunchSpec &, const QB_E *, const QB_E *, const QB_E *,
+                                                     const QB_E *, QB_E *, const GeoDev &,
+                                                     const OpDev<comp_t<QB_FT>> &, cudaStream_t);
+#endif
 template cudaError_t launch_face_unpack<QB_FT, QB_S>(int, bool, const QB_E *, const QB_E *, const QB_E *, QB_E *,
                                                      const GeoDev &, const FaceSpec &, const OpDev<comp_t<QB_FT>> &,
                                                      cudaStream_t);

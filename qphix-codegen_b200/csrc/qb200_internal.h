@@ -22,6 +22,13 @@ cudaError_t launch_dslash(const LaunchSpec &ls, const elem_t<FT> *psi, const ele
                           const elem_t<FT> *gauge, const elem_t<FT> *clov, elem_t<FT> *out, const GeoDev &g,
                           const OpDev<comp_t<FT>> &p, cudaStream_t st);
 
+// multi-RHS body kernel launcher (g.nrhs right-hand sides interleaved
+// innermost), defined in qb200_inst.cu for FT in {float, __half}, S in {4, 8, 16}
+template <typename FT, int S>
+cudaError_t launch_dslash_mrhs(const LaunchSpec &ls, const elem_t<FT> *psi, const elem_t<FT> *chi,
+                               const elem_t<FT> *gauge, const elem_t<FT> *clov, elem_t<FT> *out, const GeoDev &g,
+                               const OpDev<comp_t<FT>> &p, cudaStream_t st);
+
 // face launchers, defined in qb200_inst.cu for each (FT, S)
 struct FaceSpec {
   int dir, mu, coord, par, nface, cb;

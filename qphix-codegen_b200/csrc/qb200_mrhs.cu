@@ -1,0 +1,626 @@
+// qb200_mrhs.cu -- multi-right-hand-side operator, layout converters and
+// solvers.
+//
+// Layout: a multi-RHS spinor array holds nrhs fields of one checkerboard with
+// the right-hand side innermost, FT[block][3][4][2][S][nrhs] (padding blocks
+// as in the single layout).  One thread per (site, right-hand side) then reads
+// spinors fully coalesced while the nrhs threads of a site share each link and
+// clover load, so the gauge and clover bytes are paid once per nrhs solutions.
+// The reference has no multi-RHS kernels; this is an addition of the B200
+// build.  Storage types: FP32 and plain FP16; SOALEN 4, 8, 16.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "qphix_b200.h"
+#include "qb200_blas.cuh"
+#include "qb200_internal.h"
+
+namespace qb200 {
+int api_fail(int code, const char *msg);
+int api_geo(const qb200_lattice *l, GeoDev &g);
+int api_check_device();
+int api_body(const qb200_lattice *l, int fam, bool ach, int isPlus, int cb, const void *psi, const void *chi,
+             const void *gauge, const void *clov, void *out, const unsigned *accumulate, double coeff_s,
+             double coeff_t_f, double coeff_t_b, unsigned tbc_mask, const double *tbc_phases, double alpha,
+             double mu, double muinv, double rho, void *stream);
+} // namespace qb200
+
+using namespace qb200;
+
+namespace {
+
+constexpr int kMaxRhs = 16;
+
+int cuda_rc(cudaError_t e, const char *what)
+{
+  if (e == cudaSuccess) return QB200_OK;
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  return api_fail(QB200_ECUDA, m.c_str());
+}
+
+int fbytes(int ft) { return ft == QB200_F64 ? 8 : ft == QB200_F32 ? 4 : 2; }
+
+int grid_for(long long n)
+{
+  long long b = (n + 255) / 256;
+  if (b > 148 * 8) b = 148 * 8;
+  return (int)(b < 1 ? 1 : b);
+}
+
+int check_mr(const qb200_lattice *l, int nrhs)
+{
+  if (!l) return api_fail(QB200_ENULL, "lattice is NULL");
+  if (nrhs != 1 && nrhs != 2 && nrhs != 4 && nrhs != 8 && nrhs != 16)
+    return api_fail(QB200_EINVAL, "nrhs must be 1, 2, 4, 8 or 16");
+  if (l->ftype != QB200_F32 && l->ftype != QB200_F16)
+    return api_fail(QB200_ELAYOUT, "multi-RHS kernels are built for FP32 and FP16 storage");
+  if (l->soalen != 4 && l->soalen != 8 && l->soalen != 16)
+    return api_fail(QB200_ELAYOUT, "multi-RHS kernels are built for soalen 4, 8 and 16");
+  GeoDev g;
+  return api_geo(l, g);
+}
+
+// ---- dslash --------------------------------------------------------------
+
+template <typename FT>
+cudaError_t mr_body_t(const qb200_lattice *l, GeoDev g, int fam, bool ach, int isPlus, int cb, const void *psi,
+                      const void *chi, void *out, const void *gauge, const void *clov, const qb200_coeffs *c,
+                      const unsigned *acc, cudaStream_t st)
+{
+  typedef comp_t<FT> C;
+  OpDev<C> p;
+  std::memset(&p, 0, sizeof(p));
+  const double sg = ach ? -1.0 : 1.0;
+  for (int d = 0; d < 6; d++) p.beta[d] = (C)(sg * c->coeff_s);
+  p.beta[6] = (C)(sg * c->coeff_t_b);
+  p.beta[7] = (C)(sg * c->coeff_t_f);
+  p.tbound = (C)l->t_boundary;
+  p.t_edge_lo = l->t_edge_lo ? 1 : 0;
+  p.t_edge_hi = l->t_edge_hi ? 1 : 0;
+  p.tbc_mask = c->tbc_mask & 15u;
+  for (int m = 0; m < 4; m++) {
+    p.tbc[m][0] = (C)c->tbc_phases[m][0];
+    p.tbc[m][1] = (C)c->tbc_phases[m][1];
+  }
+  for (int d = 0; d < 8; d++)
+    if (!acc || acc[d]) p.acc_mask |= 1u << d;
+  p.isPlus = isPlus;
+  p.cb = cb;
+  p.alpha = (C)c->alpha;
+  p.mu = (C)c->mu;
+  p.muinv = (C)c->muinv;
+  p.rho = (C)c->rho;
+  LaunchSpec ls;
+  ls.fam = fam;
+  ls.ach = ach;
+  ls.comp12 = l->compress12 != 0;
+  typedef elem_t<FT> E;
+  const E *ps = (const E *)psi, *ch = (const E *)chi, *u = (const E *)gauge, *cl = (const E *)clov;
+  E *o = (E *)out;
+  switch (l->soalen) {
+  case 4: return launch_dslash_mrhs<FT, 4>(ls, ps, ch, u, cl, o, g, p, st);
+  case 8: return launch_dslash_mrhs<FT, 8>(ls, ps, ch, u, cl, o, g, p, st);
+  default: return launch_dslash_mrhs<FT, 16>(ls, ps, ch, u, cl, o, g, p, st);
+  }
+}
+
+int mr_body(const qb200_lattice *l, int nrhs, int fam, bool ach, int isPlus, int cb, const void *psi,
+            const void *chi, void *out, const void *gauge, const void *clov, const qb200_coeffs *c,
+            const unsigned *acc, cudaStream_t st)
+{
+  int rc = check_mr(l, nrhs);
+  if (rc) return rc;
+  if (fam < 0 || fam > 3) return api_fail(QB200_EINVAL, "family must be 0..3");
+  if (cb != 0 && cb != 1) return api_fail(QB200_EINVAL, "cb must be 0 or 1");
+  if (!psi || !out || !gauge || !c) return api_fail(QB200_ENULL, "psi, out, gauge and coefficients are required");
+  if (ach && !chi) return api_fail(QB200_ENULL, "achimbdpsi needs chi");
+  if ((fam == 1 || fam == 3) && !clov) return api_fail(QB200_ENULL, "clover field is NULL");
+  if (psi == out) return api_fail(QB200_EINVAL, "out must not alias psi");
+  if ((rc = api_check_device())) return rc;
+  GeoDev g;
+  api_geo(l, g);
+  g.nrhs = nrhs;
+  cudaError_t e = l->ftype == QB200_F32
+                      ? mr_body_t<float>(l, g, fam, ach, isPlus, cb, psi, chi, out, gauge, clov, c, acc, st)
+                      : mr_body_t<__half>(l, g, fam, ach, isPlus, cb, psi, chi, out, gauge, clov, c, acc, st);
+  return cuda_rc(e, "multi-RHS dslash launch");
+}
+
+// ---- layout converters ----------------------------------------------------
+
+struct PtrTab {
+  const void *p[kMaxRhs];
+  double scale[kMaxRhs];
+};
+
+// mrhs[blk][k][l][r] <-> field_r[blk][k][l] with conversion and scaling
+template <typename FO, typename FI, bool TO_MR>
+__global__ void __launch_bounds__(256) mr_convert_kernel(long long n, int S, int nrhs, PtrTab tab, void *mr)
+{
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(e % nrhs);
+    const long long j = e / nrhs; // element of one single-RHS field
+    if (TO_MR) {
+      const FI *src = reinterpret_cast<const FI *>(tab.p[r]);
+      reinterpret_cast<FO *>(mr)[e] = from_d<FO>(tab.scale[r] * to_d(src[j]));
+    } else {
+      FO *dst = reinterpret_cast<FO *>(const_cast<void *>(tab.p[r]));
+      dst[j] = from_d<FO>(tab.scale[r] * to_d(reinterpret_cast<const FI *>(mr)[e]));
+    }
+  }
+  (void)S;
+}
+
+template <typename FO, typename FI>
+cudaError_t mr_convert_t(bool to_mr, long long n, int S, int nrhs, const PtrTab &tab, void *mr, cudaStream_t st)
+{
+  if (to_mr) mr_convert_kernel<FO, FI, true><<<grid_for(n), 256, 0, st>>>(n, S, nrhs, tab, mr);
+  else mr_convert_kernel<FO, FI, false><<<grid_for(n), 256, 0, st>>>(n, S, nrhs, tab, mr);
+  return cudaGetLastError();
+}
+
+// single-layout fields of type ft_single <-> multi-RHS array of type ft_mr
+cudaError_t mr_convert(bool to_mr, int ft_mr, int ft_single, long long n_total, int S, int nrhs, const PtrTab &tab,
+                       void *mr, cudaStream_t st)
+{
+  // to_mr: FO = mr type, FI = single type; else FO = single type, FI = mr type
+  const int fo = to_mr ? ft_mr : ft_single, fi = to_mr ? ft_single : ft_mr;
+#define QB_CV(A, B) return mr_convert_t<A, B>(to_mr, n_total, S, nrhs, tab, mr, st)
+  if (fo == QB200_F32 && fi == QB200_F32) QB_CV(float, float);
+  if (fo == QB200_F32 && fi == QB200_F64) QB_CV(float, double);
+  if (fo == QB200_F64 && fi == QB200_F32) QB_CV(double, float);
+  if (fo == QB200_F16 && fi == QB200_F16) QB_CV(__half, __half);
+  if (fo == QB200_F16 && fi == QB200_F64) QB_CV(__half, double);
+  if (fo == QB200_F64 && fi == QB200_F16) QB_CV(double, __half);
+  if (fo == QB200_F16 && fi == QB200_F32) QB_CV(__half, float);
+  if (fo == QB200_F32 && fi == QB200_F16) QB_CV(float, __half);
+#undef QB_CV
+  return cudaErrorInvalidValue;
+}
+
+// one single-layout field <-> slot `slot` of a multi-RHS array, with scaling
+template <typename FO, typename FI, bool TO_MR>
+__global__ void __launch_bounds__(256) mr_slot_kernel(long long n1, int nrhs, int slot, const void *__restrict__ in,
+                                                      double scale, void *__restrict__ out)
+{
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n1;
+       j += (long long)gridDim.x * blockDim.x) {
+    if (TO_MR)
+      reinterpret_cast<FO *>(out)[j * nrhs + slot] = from_d<FO>(scale * to_d(reinterpret_cast<const FI *>(in)[j]));
+    else
+      reinterpret_cast<FO *>(out)[j] = from_d<FO>(scale * to_d(reinterpret_cast<const FI *>(in)[j * nrhs + slot]));
+  }
+}
+
+// FP64 single field -> slot of an FP32/FP16 multi-RHS array (TO_MR), or back
+cudaError_t mr_slot(bool to_mr, int ft_mr, long long n1, int nrhs, int slot, const void *in, double scale, void *out,
+                    cudaStream_t st)
+{
+  const int gr = grid_for(n1);
+  if (to_mr) {
+    if (ft_mr == QB200_F32) mr_slot_kernel<float, double, true><<<gr, 256, 0, st>>>(n1, nrhs, slot, in, scale, out);
+    else mr_slot_kernel<__half, double, true><<<gr, 256, 0, st>>>(n1, nrhs, slot, in, scale, out);
+  } else {
+    if (ft_mr == QB200_F32) mr_slot_kernel<double, float, false><<<gr, 256, 0, st>>>(n1, nrhs, slot, in, scale, out);
+    else mr_slot_kernel<double, __half, false><<<gr, 256, 0, st>>>(n1, nrhs, slot, in, scale, out);
+  }
+  return cudaGetLastError();
+}
+
+// ---- per-RHS BLAS on the multi-RHS layout -----------------------------------
+
+// a[r] = sign * num[r] / den[r] (0 when den[r] == 0), or host[r]
+struct VecScalar {
+  const double *num, *den;
+  double sign;
+  double host[kMaxRhs];
+  __device__ __forceinline__ double get(int r) const
+  {
+    if (!num) return host[r];
+    const double d = den ? den[r] : 1.0;
+    return d == 0.0 ? 0.0 : sign * num[r] / d;
+  }
+};
+
+template <typename FT>
+__global__ void __launch_bounds__(256) mr_axpby_kernel(long long n, int nrhs, VecScalar a, const FT *__restrict__ x,
+                                                       VecScalar b, FT *__restrict__ y)
+{
+  const long long stride = (long long)gridDim.x * blockDim.x; // a multiple of nrhs
+  const long long e0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int r = (int)(e0 % nrhs);
+  const double av = a.get(r), bv = b.get(r);
+  for (long long e = e0; e < n; e += stride) y[e] = from_d<FT>(av * to_d(x[e]) + bv * to_d(y[e]));
+}
+
+// partials[r*kRedBlocks + block] = sum over the block's elements of rhs r
+template <typename FT>
+__global__ void __launch_bounds__(kRedThreads) mr_dot_kernel(long long n, int nrhs, const FT *__restrict__ x,
+                                                             const FT *__restrict__ y, double *__restrict__ partials)
+{
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long e0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double s = 0.0;
+  for (long long e = e0; e < n; e += stride) s += to_d(x[e]) * to_d(y[e]);
+  // lanes with equal lane % nrhs hold the same right-hand side
+  for (int o = 16; o >= nrhs; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __shared__ double sh[kRedThreads / 32][kMaxRhs];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l < nrhs) sh[w][l] = s;
+  __syncthreads();
+  if (threadIdx.x < nrhs) {
+    double t = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); i++) t += sh[i][threadIdx.x];
+    partials[threadIdx.x * kRedBlocks + blockIdx.x] = t;
+  }
+}
+
+__global__ void mr_finish_kernel(const double *__restrict__ partials, int nrhs, double *__restrict__ result)
+{
+  const int r = blockIdx.x;
+  double s = 0.0, dummy = 0.0;
+  for (int i = threadIdx.x; i < kRedBlocks; i += blockDim.x) s += partials[r * kRedBlocks + i];
+  block_sum2(s, dummy);
+  if (threadIdx.x == 0) result[r] = s;
+  (void)nrhs;
+}
+
+VecScalar vhost(double v)
+{
+  VecScalar s;
+  s.num = s.den = nullptr;
+  s.sign = 1.0;
+  for (int r = 0; r < kMaxRhs; r++) s.host[r] = v;
+  return s;
+}
+
+VecScalar vratio(const double *num, const double *den, double sign)
+{
+  VecScalar s = vhost(0.0);
+  s.num = num;
+  s.den = den;
+  s.sign = sign;
+  return s;
+}
+
+struct MR {
+  int ft, nrhs;
+  long long n; // total elements
+};
+
+cudaError_t mr_axpby(const MR &m, VecScalar a, const void *x, VecScalar b, void *y, cudaStream_t st)
+{
+  // a grid stride that is a multiple of nrhs keeps each thread on one rhs
+  const int blocks = 148 * 4;
+  if (m.ft == QB200_F32) mr_axpby_kernel<float><<<blocks, 256, 0, st>>>(m.n, m.nrhs, a, (const float *)x, b, (float *)y);
+  else if (m.ft == QB200_F64)
+    mr_axpby_kernel<double><<<blocks, 256, 0, st>>>(m.n, m.nrhs, a, (const double *)x, b, (double *)y);
+  else mr_axpby_kernel<__half><<<blocks, 256, 0, st>>>(m.n, m.nrhs, a, (const __half *)x, b, (__half *)y);
+  return cudaGetLastError();
+}
+
+cudaError_t mr_dot(const MR &m, const void *x, const void *y, double *partials, double *result, cudaStream_t st)
+{
+  if (m.ft == QB200_F32)
+    mr_dot_kernel<float><<<kRedBlocks, kRedThreads, 0, st>>>(m.n, m.nrhs, (const float *)x, (const float *)y, partials);
+  else if (m.ft == QB200_F64)
+    mr_dot_kernel<double><<<kRedBlocks, kRedThreads, 0, st>>>(m.n, m.nrhs, (const double *)x, (const double *)y,
+                                                               partials);
+  else
+    mr_dot_kernel<__half><<<kRedBlocks, kRedThreads, 0, st>>>(m.n, m.nrhs, (const __half *)x, (const __half *)y,
+                                                               partials);
+  mr_finish_kernel<<<m.nrhs, kRedThreads, 0, st>>>(partials, m.nrhs, result);
+  return cudaGetLastError();
+}
+
+// ---- operator and solver ---------------------------------------------------
+
+qb200_coeffs coeffs_of(const qb200_operator *op, double scale)
+{
+  qb200_coeffs c;
+  c.coeff_s = op->coeff_s * scale;
+  c.coeff_t_f = op->coeff_t_f * scale;
+  c.coeff_t_b = op->coeff_t_b * scale;
+  c.alpha = op->alpha;
+  c.mu = op->mu;
+  c.muinv = op->muinv;
+  c.rho = op->rho;
+  c.tbc_mask = op->tbc_mask;
+  std::memcpy(c.tbc_phases, op->tbc_phases, sizeof(c.tbc_phases));
+  return c;
+}
+
+int check_op(const qb200_operator *op)
+{
+  if (!op) return api_fail(QB200_ENULL, "operator is NULL");
+  if (op->family < 0 || op->family > 3) return api_fail(QB200_EINVAL, "operator family must be 0..3");
+  if (op->target_cb != 0 && op->target_cb != 1) return api_fail(QB200_EINVAL, "target_cb must be 0 or 1");
+  if (!op->gauge[0] || !op->gauge[1]) return api_fail(QB200_ENULL, "both gauge checkerboards are needed");
+  if ((op->family == 1 || op->family == 3) && (!op->clov[0] || !op->clov[1]))
+    return api_fail(QB200_ENULL, "clover operator needs both clover checkerboards");
+  if (op->family == 3 && (!op->clov_dag[0] || !op->clov_dag[1]))
+    return api_fail(QB200_ENULL, "twisted-mass clover dagger needs clov_dag");
+  if (op->family == 0 && op->alpha == 0.0) return api_fail(QB200_EINVAL, "Wilson operator needs alpha != 0");
+  return QB200_OK;
+}
+
+// out = Mhat in (or Mhat^dag) on nrhs right-hand sides
+int mr_schur(const qb200_lattice *l, int nrhs, const qb200_operator *op, int isPlus, const void *in, void *out,
+             void *tmp, cudaStream_t st)
+{
+  const int tc = op->target_cb, oc = 1 - tc;
+  const void *clov_o = op->clov[oc], *clov_t = op->clov[tc];
+  if (op->family == 3 && !isPlus) {
+    clov_o = op->clov_dag[oc];
+    clov_t = op->clov_dag[tc];
+  }
+  const qb200_coeffs c1 = coeffs_of(op, op->family == 0 ? 1.0 / op->alpha : 1.0);
+  int rc = mr_body(l, nrhs, op->family, false, isPlus, oc, in, nullptr, tmp, op->gauge[oc], clov_o, &c1, nullptr, st);
+  if (rc) return rc;
+  const qb200_coeffs c2 = coeffs_of(op, 1.0);
+  return mr_body(l, nrhs, op->family, true, isPlus, tc, tmp, in, out, op->gauge[tc], clov_t, &c2, nullptr, st);
+}
+
+size_t single_bytes(const qb200_lattice *l) { return (size_t)qb200_spinor_elems(l) * fbytes(l->ftype); }
+
+size_t ws_bytes(const qb200_lattice *l, int nrhs, int nspin)
+{
+  if (qb200_spinor_elems(l) < 0) return 0;
+  return nspin * (single_bytes(l) * nrhs + 256) + (size_t)(kRedBlocks * kMaxRhs + 16 * kMaxRhs) * 8 + 4096;
+}
+
+struct Work {
+  char *p;
+  size_t off;
+  void *take(size_t b)
+  {
+    off = (off + 255) & ~(size_t)255;
+    void *r = p + off;
+    off += b;
+    return r;
+  }
+};
+
+struct MRVecs {
+  void *v[10];
+  double *partials, *scal; // scal: 16 slots of kMaxRhs doubles
+  double *slot(int k) { return scal + k * kMaxRhs; }
+};
+
+MRVecs mr_carve(const qb200_lattice *l, int nrhs, void *ws, int nspin)
+{
+  Work w{(char *)ws, 0};
+  MRVecs m;
+  for (int i = 0; i < nspin && i < 10; i++) m.v[i] = w.take(single_bytes(l) * nrhs);
+  m.partials = (double *)w.take((size_t)kRedBlocks * kMaxRhs * 8);
+  m.scal = (double *)w.take((size_t)16 * kMaxRhs * 8);
+  return m;
+}
+
+int fetch(double *h, const double *d, int n, cudaStream_t st)
+{
+  cudaError_t e = cudaMemcpyAsync(h, d, n * sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  return cuda_rc(e, "reduction readback");
+}
+
+// CG on Mhat^dag Mhat for nrhs systems at once (independent recurrences,
+// shared operator applications).  ws vectors: r, p, Ap, t, tmp.
+int mr_cg_core(const qb200_lattice *l, int nrhs, const qb200_operator *op, const void *rhs, void *x, double tol,
+               int max_iter, MRVecs &s, int *iters, double *rel, cudaStream_t st)
+{
+  MR m;
+  m.ft = l->ftype;
+  m.nrhs = nrhs;
+  m.n = qb200_spinor_elems(l) * nrhs;
+  const size_t bytes = single_bytes(l) * nrhs;
+  void *r = s.v[0], *p = s.v[1], *Ap = s.v[2], *t = s.v[3], *tmp = s.v[4];
+  double *rr = s.slot(0), *rrn = s.slot(1), *pAp = s.slot(2), *bb = s.slot(3);
+  int rc;
+  if ((rc = mr_schur(l, nrhs, op, 1, x, t, tmp, st))) return rc;
+  if ((rc = mr_schur(l, nrhs, op, 0, t, Ap, tmp, st))) return rc;
+  cudaError_t e = cudaMemcpyAsync(r, rhs, bytes, cudaMemcpyDeviceToDevice, st);
+  if (e == cudaSuccess) e = mr_axpby(m, vhost(-1.0), Ap, vhost(1.0), r, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(p, r, bytes, cudaMemcpyDeviceToDevice, st);
+  if (e == cudaSuccess) e = mr_dot(m, r, r, s.partials, rr, st);
+  if (e == cudaSuccess) e = mr_dot(m, rhs, rhs, s.partials, bb, st);
+  if ((rc = cuda_rc(e, "multi-RHS cg setup"))) return rc;
+  double h_rr[kMaxRhs], h_bb[kMaxRhs];
+  if ((rc = fetch(h_bb, bb, nrhs, st))) return rc;
+  if ((rc = fetch(h_rr, rr, nrhs, st))) return rc;
+  auto done = [&]() {
+    for (int i = 0; i < nrhs; i++)
+      if (h_rr[i] > tol * tol * h_bb[i]) return false;
+    return true;
+  };
+  int k = 0;
+  while (!done() && k < max_iter) {
+    if ((rc = mr_schur(l, nrhs, op, 1, p, t, tmp, st))) return rc;
+    if ((rc = mr_schur(l, nrhs, op, 0, t, Ap, tmp, st))) return rc;
+    e = mr_dot(m, p, Ap, s.partials, pAp, st);
+    if (e == cudaSuccess) e = mr_axpby(m, vratio(rr, pAp, 1.0), p, vhost(1.0), x, st);
+    if (e == cudaSuccess) e = mr_axpby(m, vratio(rr, pAp, -1.0), Ap, vhost(1.0), r, st);
+    if (e == cudaSuccess) e = mr_dot(m, r, r, s.partials, rrn, st);
+    if (e == cudaSuccess) e = mr_axpby(m, vhost(1.0), r, vratio(rrn, rr, 1.0), p, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(rr, rrn, nrhs * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    if ((rc = cuda_rc(e, "multi-RHS cg iteration"))) return rc;
+    if ((rc = fetch(h_rr, rr, nrhs, st))) return rc;
+    k++;
+    for (int i = 0; i < nrhs; i++)
+      if (!std::isfinite(h_rr[i])) return api_fail(QB200_EINVAL, "multi-RHS cg: residual is not finite");
+  }
+  *iters = k;
+  for (int i = 0; i < nrhs; i++) rel[i] = h_bb[i] > 0 ? std::sqrt(h_rr[i] / h_bb[i]) : 0.0;
+  return QB200_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+long long qb200_mrhs_spinor_elems(const qb200_lattice *lat, int nrhs)
+{
+  const long long n = qb200_spinor_elems(lat);
+  return n < 0 || nrhs < 1 ? -1 : n * nrhs;
+}
+
+int qb200_mrhs_pack(const qb200_lattice *lat, int nrhs, const void *const *fields, void *mrhs, void *stream)
+{
+  int rc = check_mr(lat, nrhs);
+  if (rc) return rc;
+  if (!fields || !mrhs) return api_fail(QB200_ENULL, "fields and mrhs must be non-NULL");
+  PtrTab tab;
+  for (int r = 0; r < nrhs; r++) {
+    if (!fields[r]) return api_fail(QB200_ENULL, "a field pointer is NULL");
+    tab.p[r] = fields[r];
+    tab.scale[r] = 1.0;
+  }
+  const long long n = qb200_spinor_elems(lat) * nrhs;
+  return cuda_rc(mr_convert(true, lat->ftype, lat->ftype, n, lat->soalen, nrhs, tab, mrhs, (cudaStream_t)stream),
+                 "multi-RHS pack");
+}
+
+int qb200_mrhs_unpack(const qb200_lattice *lat, int nrhs, const void *mrhs, void *const *fields, void *stream)
+{
+  int rc = check_mr(lat, nrhs);
+  if (rc) return rc;
+  if (!fields || !mrhs) return api_fail(QB200_ENULL, "fields and mrhs must be non-NULL");
+  PtrTab tab;
+  for (int r = 0; r < nrhs; r++) {
+    if (!fields[r]) return api_fail(QB200_ENULL, "a field pointer is NULL");
+    tab.p[r] = fields[r];
+    tab.scale[r] = 1.0;
+  }
+  const long long n = qb200_spinor_elems(lat) * nrhs;
+  return cuda_rc(mr_convert(false, lat->ftype, lat->ftype, n, lat->soalen, nrhs, tab, const_cast<void *>(mrhs),
+                            (cudaStream_t)stream),
+                 "multi-RHS unpack");
+}
+
+int qb200_dslash_mrhs(const qb200_lattice *lat, int nrhs, int family, int achimbdpsi, int isign, int cb,
+                      const void *psi, const void *chi, void *out, const void *gauge, const void *clover,
+                      const qb200_coeffs *coeffs, const unsigned accumulate[8], void *stream)
+{
+  return mr_body(lat, nrhs, family, achimbdpsi != 0, isign > 0, cb, psi, chi, out, gauge, clover, coeffs,
+                 accumulate, (cudaStream_t)stream);
+}
+
+int qb200_schur_apply_mrhs(const qb200_lattice *lat, int nrhs, const qb200_operator *op, int isign, const void *in,
+                           void *out, void *tmp_other_cb, void *stream)
+{
+  int rc = check_mr(lat, nrhs);
+  if (rc) return rc;
+  if ((rc = check_op(op))) return rc;
+  if (!in || !out || !tmp_other_cb) return api_fail(QB200_ENULL, "in, out and tmp must be non-NULL");
+  return mr_schur(lat, nrhs, op, isign > 0, in, out, tmp_other_cb, (cudaStream_t)stream);
+}
+
+long long qb200_cg_mrhs_workspace_bytes(const qb200_lattice *lat, int nrhs) { return (long long)ws_bytes(lat, nrhs, 6); }
+
+int qb200_invert_cg_mrhs(const qb200_lattice *lat, int nrhs, const qb200_operator *op, const void *b, void *x,
+                         double rel_tol, int max_iter, void *workspace, int *iters, double *rel_res, void *stream)
+{
+  int rc = check_mr(lat, nrhs);
+  if (rc) return rc;
+  if ((rc = check_op(op))) return rc;
+  if (!b || !x || !workspace || !rel_res) return api_fail(QB200_ENULL, "b, x, workspace and rel_res are required");
+  cudaStream_t st = (cudaStream_t)stream;
+  MRVecs s = mr_carve(lat, nrhs, workspace, 6);
+  void *rhs = s.v[5];
+  if ((rc = mr_schur(lat, nrhs, op, 0, b, rhs, s.v[4], st))) return rc;
+  int k = 0;
+  if ((rc = mr_cg_core(lat, nrhs, op, rhs, x, rel_tol, max_iter, s, &k, rel_res, st))) return rc;
+  if (iters) *iters = k;
+  return QB200_OK;
+}
+
+long long qb200_mixed_mrhs_workspace_bytes(const qb200_lattice *lat_hi, const qb200_lattice *lat_lo, int nrhs,
+                                           long long *lo_bytes)
+{
+  if (lo_bytes) *lo_bytes = (long long)ws_bytes(lat_lo, nrhs, 8);
+  return (long long)ws_bytes(lat_hi, 1, 4);
+}
+
+// Defect correction for nrhs systems: per right-hand side the true residual
+// b_i - Mhat x_i is formed with the single-RHS FP64 operator (op_hi), the
+// normal-equation residuals are packed, scaled to O(1), into one multi-RHS
+// array of the low precision, solved together with the multi-RHS low
+// precision operator (op_lo, FP16 or FP32 storage) to inner_tol, and the
+// corrections are accumulated in FP64.  b and x: host arrays of nrhs device
+// pointers to FP64 single-layout spinors.
+int qb200_invert_mixed_mrhs(const qb200_lattice *lat_hi, const qb200_operator *op_hi, const qb200_lattice *lat_lo,
+                            const qb200_operator *op_lo, int nrhs, const void *const *b, void *const *x,
+                            double rel_tol, double inner_tol, int max_inner, int max_outer, void *ws_hi, void *ws_lo,
+                            int *inner_iters, int *outer_iters, double *rel_res, void *stream)
+{
+  int rc = check_mr(lat_lo, nrhs);
+  if (rc) return rc;
+  if ((rc = check_op(op_hi)) || (rc = check_op(op_lo))) return rc;
+  if (!lat_hi || lat_hi->ftype != QB200_F64) return api_fail(QB200_EINVAL, "the high precision lattice must be FP64");
+  if (!b || !x || !ws_hi || !ws_lo || !rel_res) return api_fail(QB200_ENULL, "missing argument");
+  if (qb200_spinor_elems(lat_hi) != qb200_spinor_elems(lat_lo))
+    return api_fail(QB200_EINVAL, "high and low precision lattices differ in shape");
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long n1 = qb200_spinor_elems(lat_hi);
+  Work wh{(char *)ws_hi, 0};
+  void *r = wh.take(n1 * 8), *rn = wh.take(n1 * 8), *ehi = wh.take(n1 * 8), *tmp = wh.take(n1 * 8);
+  double *partials = (double *)wh.take((size_t)kRedBlocks * 2 * 8);
+  double *scal = (double *)wh.take(64 * 8);
+  MRVecs L = mr_carve(lat_lo, nrhs, ws_lo, 8);
+  void *rhs_lo = L.v[6], *e_lo = L.v[7];
+  const size_t lo_bytes = single_bytes(lat_lo) * nrhs;
+  for (int i = 0; i < nrhs; i++)
+    if ((rc = cuda_rc(cudaMemsetAsync(x[i], 0, n1 * 8, st), "mixed init"))) return rc;
+  double bnorm[kMaxRhs], scale[kMaxRhs], rel[kMaxRhs];
+  for (int i = 0; i < nrhs; i++) {
+    if ((rc = qb200_blas_dot(QB200_F64, n1, b[i], b[i], scal, partials, st))) return rc;
+    if ((rc = fetch(&bnorm[i], scal, 1, st))) return rc;
+  }
+  int tot = 0, outer = 0;
+  while (true) {
+    bool all = true;
+    for (int i = 0; i < nrhs; i++) {
+      // r = b_i - Mhat x_i ; rn = Mhat^dag r
+      if ((rc = qb200_schur_apply(lat_hi, op_hi, 1, x[i], r, tmp, st))) return rc;
+      if ((rc = qb200_blas_axpby(QB200_F64, n1, 1.0, b[i], -1.0, r, st))) return rc;
+      double rr;
+      if ((rc = qb200_blas_dot(QB200_F64, n1, r, r, scal, partials, st))) return rc;
+      if ((rc = fetch(&rr, scal, 1, st))) return rc;
+      rel[i] = bnorm[i] > 0 ? std::sqrt(rr / bnorm[i]) : 0.0;
+      if (rel[i] > rel_tol) all = false;
+      // the normal residual goes to the low-precision pack through a staging
+      // buffer per rhs: stage in ehi (rn of this rhs), convert below
+      if ((rc = qb200_schur_apply(lat_hi, op_hi, -1, r, rn, tmp, st))) return rc;
+      double rnn;
+      if ((rc = qb200_blas_dot(QB200_F64, n1, rn, rn, scal, partials, st))) return rc;
+      if ((rc = fetch(&rnn, scal, 1, st))) return rc;
+      scale[i] = std::sqrt((double)n1 / (rnn > 0 ? rnn : 1.0));
+      // the scaled normal residual becomes slot i of the low-precision rhs
+      if ((rc = cuda_rc(mr_slot(true, lat_lo->ftype, n1, nrhs, i, rn, scale[i], rhs_lo, st), "multi-RHS pack slot")))
+        return rc;
+    }
+    if (all || outer >= max_outer) break;
+    if ((rc = cuda_rc(cudaMemsetAsync(e_lo, 0, lo_bytes, st), "mixed zero"))) return rc;
+    int k = 0;
+    double irel[kMaxRhs];
+    if ((rc = mr_cg_core(lat_lo, nrhs, op_lo, rhs_lo, e_lo, inner_tol, max_inner, L, &k, irel, st))) return rc;
+    tot += k;
+    for (int i = 0; i < nrhs; i++) {
+      if ((rc = cuda_rc(mr_slot(false, lat_lo->ftype, n1, nrhs, i, e_lo, 1.0 / scale[i], ehi, st),
+                        "multi-RHS unpack slot")))
+        return rc;
+      if ((rc = qb200_blas_axpby(QB200_F64, n1, 1.0, ehi, 1.0, x[i], st))) return rc;
+    }
+    outer++;
+  }
+  if (inner_iters) *inner_iters = tot;
+  if (outer_iters) *outer_iters = outer;
+  for (int i = 0; i < nrhs; i++) rel_res[i] = rel[i];
+  return QB200_OK;
+}
+
+} // extern "C"

@@ -19,10 +19,10 @@ template <typename FT> struct KArgs {
   elem_t<FT> *out;
 };
 
-template <typename FT, int S, bool COMP12, int D>
+template <typename FT, int S, bool COMP12, int D, bool MR>
 __device__ __forceinline__ void do_hop(const KArgs<FT> &a, const GeoDev &g,
                                        const OpDev<typename ftraits<FT>::C> &p, const Site &s,
-                                       long long gbase,
+                                       long long gbase, int rhs,
                                        cx<typename ftraits<FT>::C> (&acc)[4][3])
 {
   typedef typename ftraits<FT>::C C;
@@ -36,7 +36,8 @@ __device__ __forceinline__ void do_hop(const KArgs<FT> &a, const GeoDev &g,
   if (D == 7 && s.t == g.nt - 1 && p.t_edge_hi) beta *= p.tbound;
 
   cx<C> psi[4][3], b[2][3], ub[2][3], G[3][3];
-  load_spinor<FT, S>(a.psi, spinor_base<FT, S>(g, n), psi);
+  if (MR) load_spinor_rs<FT>(a.psi, spinor_base_mr<S>(g, n, rhs), S * g.nrhs, psi);
+  else load_spinor<FT, S>(a.psi, spinor_base<FT, S>(g, n), psi);
   const C sigma = p.isPlus ? (C)1 : (C)-1;
   project<C, D>(psi, sigma, b);
   load_link<FT, COMP12, D>(a.gauge, gbase, g.V, G);
@@ -51,19 +52,25 @@ __device__ __forceinline__ void do_hop(const KArgs<FT> &a, const GeoDev &g,
   recons<C, MU>(ub, beta, tau, acc);
 }
 
-template <typename FT, int S, bool COMP12, int FAM, bool ACH>
+// MR: multi-RHS layout, one thread per (site, right-hand side) with the
+// right-hand side fastest, so the nrhs threads of a site share each link and
+// clover load
+template <typename FT, int S, bool COMP12, int FAM, bool ACH, bool MR>
 __global__ void __launch_bounds__(128)
     site_dslash_kernel(const KArgs<FT> a, const GeoDev g, const OpDev<typename ftraits<FT>::C> p)
 {
   typedef typename ftraits<FT>::C C;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= g.nsites) return;
+  const int gi = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gi >= g.nsites * (MR ? g.nrhs : 1)) return;
+  const int i = MR ? gi / g.nrhs : gi;
+  const int rhs = MR ? gi - i * g.nrhs : 0;
   const Site s = site_of(g, i, p.cb);
   int lane;
   const long long tile = tile_of<S>(g, s, &lane);
   constexpr int R = COMP12 ? 2 : 3;
   const long long gbase = tile * (8LL * R * 6 * g.V) + lane;
-  const long long obase = spinor_base<FT, S>(g, s);
+  const long long obase = MR ? spinor_base_mr<S>(g, s, rhs) : spinor_base<FT, S>(g, s);
+  const int cs = S * g.nrhs;
 
   cx<C> res[4][3];
   cx<C> acc[4][3];
@@ -76,7 +83,8 @@ __global__ void __launch_bounds__(128)
     // A.chi first (achiResult, dslash_common.cc:1559-1655), then the hops are
     // subtracted (beta already negated by the host)
     cx<C> ch[4][3];
-    load_spinor<FT, S>(a.chi, obase, ch);
+    if (MR) load_spinor_rs<FT>(a.chi, obase, cs, ch);
+    else load_spinor<FT, S>(a.chi, obase, ch);
     if (FAM == FAM_WILSON) {
 #pragma unroll
       for (int sp = 0; sp < 4; sp++)
@@ -110,27 +118,27 @@ __global__ void __launch_bounds__(128)
         }
       }
     }
-    do_hop<FT, S, COMP12, 0>(a, g, p, s, gbase, res);
-    do_hop<FT, S, COMP12, 1>(a, g, p, s, gbase, res);
-    do_hop<FT, S, COMP12, 2>(a, g, p, s, gbase, res);
-    do_hop<FT, S, COMP12, 3>(a, g, p, s, gbase, res);
-    do_hop<FT, S, COMP12, 4>(a, g, p, s, gbase, res);
-    do_hop<FT, S, COMP12, 5>(a, g, p, s, gbase, res);
-    do_hop<FT, S, COMP12, 6>(a, g, p, s, gbase, res);
-    do_hop<FT, S, COMP12, 7>(a, g, p, s, gbase, res);
+    do_hop<FT, S, COMP12, 0, MR>(a, g, p, s, gbase, rhs, res);
+    do_hop<FT, S, COMP12, 1, MR>(a, g, p, s, gbase, rhs, res);
+    do_hop<FT, S, COMP12, 2, MR>(a, g, p, s, gbase, rhs, res);
+    do_hop<FT, S, COMP12, 3, MR>(a, g, p, s, gbase, rhs, res);
+    do_hop<FT, S, COMP12, 4, MR>(a, g, p, s, gbase, rhs, res);
+    do_hop<FT, S, COMP12, 5, MR>(a, g, p, s, gbase, rhs, res);
+    do_hop<FT, S, COMP12, 6, MR>(a, g, p, s, gbase, rhs, res);
+    do_hop<FT, S, COMP12, 7, MR>(a, g, p, s, gbase, rhs, res);
   } else {
 #pragma unroll
     for (int sp = 0; sp < 4; sp++)
 #pragma unroll
       for (int c = 0; c < 3; c++) acc[sp][c] = mk<C>(0, 0);
-    do_hop<FT, S, COMP12, 0>(a, g, p, s, gbase, acc);
-    do_hop<FT, S, COMP12, 1>(a, g, p, s, gbase, acc);
-    do_hop<FT, S, COMP12, 2>(a, g, p, s, gbase, acc);
-    do_hop<FT, S, COMP12, 3>(a, g, p, s, gbase, acc);
-    do_hop<FT, S, COMP12, 4>(a, g, p, s, gbase, acc);
-    do_hop<FT, S, COMP12, 5>(a, g, p, s, gbase, acc);
-    do_hop<FT, S, COMP12, 6>(a, g, p, s, gbase, acc);
-    do_hop<FT, S, COMP12, 7>(a, g, p, s, gbase, acc);
+    do_hop<FT, S, COMP12, 0, MR>(a, g, p, s, gbase, rhs, acc);
+    do_hop<FT, S, COMP12, 1, MR>(a, g, p, s, gbase, rhs, acc);
+    do_hop<FT, S, COMP12, 2, MR>(a, g, p, s, gbase, rhs, acc);
+    do_hop<FT, S, COMP12, 3, MR>(a, g, p, s, gbase, rhs, acc);
+    do_hop<FT, S, COMP12, 4, MR>(a, g, p, s, gbase, rhs, acc);
+    do_hop<FT, S, COMP12, 5, MR>(a, g, p, s, gbase, rhs, acc);
+    do_hop<FT, S, COMP12, 6, MR>(a, g, p, s, gbase, rhs, acc);
+    do_hop<FT, S, COMP12, 7, MR>(a, g, p, s, gbase, rhs, acc);
     if (FAM == FAM_CLOVER || FAM == FAM_TMCLOV) {
       const long long cbase = tile * ((FAM == FAM_CLOVER ? 72LL : 144LL) * g.V) + lane;
 #pragma unroll
@@ -147,7 +155,8 @@ __global__ void __launch_bounds__(128)
         for (int c = 0; c < 3; c++) res[sp][c] = acc[sp][c];
     }
   }
-  store_spinor<FT, S>(a.out, obase, res);
+  if (MR) store_spinor_rs<FT>(a.out, obase, cs, res);
+  else store_spinor<FT, S>(a.out, obase, res);
 }
 
 } // namespace qb200

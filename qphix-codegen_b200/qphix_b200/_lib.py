@@ -96,6 +96,33 @@ INFO.update({
     "qb200_mixed_workspace_bytes": ([_LAT, _LAT, ctypes.POINTER(_LL)], _LL),
 })
 
+
+
+class Coeffs(ctypes.Structure):
+    """ctypes mirror of `qb200_coeffs`."""
+    _fields_ = [
+        ("coeff_s", ctypes.c_double), ("coeff_t_f", ctypes.c_double), ("coeff_t_b", ctypes.c_double),
+        ("alpha", ctypes.c_double), ("mu", ctypes.c_double), ("muinv", ctypes.c_double), ("rho", ctypes.c_double),
+        ("tbc_mask", ctypes.c_uint), ("tbc_phases", (ctypes.c_double * 2) * 4),
+    ]
+
+
+_PP = ctypes.POINTER(ctypes.c_void_p)
+SIGNATURES.update({
+    "qb200_spinor_convert": [_LAT, _P, _LAT, _P, _D, _P],
+    "qb200_mrhs_pack": [_LAT, _I, _PP, _P, _P],
+    "qb200_mrhs_unpack": [_LAT, _I, _P, _PP, _P],
+    "qb200_dslash_mrhs": [_LAT, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, ctypes.POINTER(Coeffs), _UA, _P],
+    "qb200_schur_apply_mrhs": [_LAT, _I, _OP, _I, _P, _P, _P, _P],
+    "qb200_invert_cg_mrhs": [_LAT, _I, _OP, _P, _P, _D, _I, _P, _IP, _DP, _P],
+    "qb200_invert_mixed_mrhs": [_LAT, _OP, _LAT, _OP, _I, _PP, _PP, _D, _D, _I, _I, _P, _P, _IP, _IP, _DP, _P],
+})
+INFO.update({
+    "qb200_mrhs_spinor_elems": ([_LAT, _I], _LL),
+    "qb200_cg_mrhs_workspace_bytes": ([_LAT, _I], _LL),
+    "qb200_mixed_mrhs_workspace_bytes": ([_LAT, _LAT, _I, ctypes.POINTER(_LL)], _LL),
+})
+
 _lib = None
 
 
