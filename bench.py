@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bound of the CPU baseline sample")
+    ap.add_argument("--no-extras", action="store_true", help="skip the multi-RHS and solver measurements")
     return ap.parse_args()
 
 
@@ -206,6 +207,94 @@ def run_reference_cpu(dims, steps, warmup, seconds, fields_gpu=None, g_gpu=None)
 
 # ---------------------------------------------------------------------------
 
+def _time(fn, reps, stream):
+    for _ in range(3):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def bench_mrhs(g, f, dev):
+    """Multi-RHS clover A.chi - b.D.psi: nrhs right-hand sides share one link
+    and clover field; per right-hand-side site 288 + 672/nrhs bytes."""
+    from qphix_b200 import mrhs
+    res = {}
+    stream = torch.cuda.current_stream()
+    for n in (4, 8, 16):
+        psi = torch.randn(g.spinor_elems * n, device=dev)
+        chi = torch.randn(g.spinor_elems * n, device=dev)
+        out = torch.zeros_like(psi)
+        ms = _time(lambda: mrhs.dslash(g, n, "clover", "achimbdpsi", 1, 0, psi, out, f["gauge"], chi=chi,
+                                       clover=f["clover"], **PARAMS), 20, stream)
+        bps = 3 * 96 + (384 + 288) / n
+        res["nrhs_%d" % n] = {"ms_per_call": ms, "gflops": FLOP_SITE * g.vol_cb * n / (ms * 1e-3) / 1e9,
+                              "gbs": bps * g.vol_cb * n / (ms * 1e-3) / 1e9, "bytes_per_rhs_site": bps}
+        del psi, chi, out
+    res["note"] = "GB/s against 288 + 672/nrhs algorithmic bytes per right-hand-side site"
+    return res
+
+
+def bench_solve(dims, dev, nrhs=8, kappa=0.16):
+    """Even-odd clover system (b = kappa = 0.16, the kappa of the twisted-mass
+    configuration) on the bench lattice solved to |b - Mhat x|/|b| <= 1e-10
+    for nrhs Gaussian sources: (a) one FP64 CG per source, (b) FP32-corrected-
+    by-FP64 CG per source, (c) all sources at once with FP16-storage multi-RHS
+    corrections of FP64 solutions.  Each path runs once untimed first (module
+    loading, workspaces), then timed."""
+    from qphix_b200 import fields, layout, mrhs
+    from qphix_b200.lattice import F16, F32, F64, Geometry
+    from qphix_b200.solver import EvenOddOperator, mixed_solve
+    G = Geometry(*dims, soalen=16, compress12=True, t_boundary=-1.0, ftype=F64)
+    U = fields.random_gauge(G, seed=77, device=dev)
+    gauge = [layout.pack_gauge(G, U, cb, torch.float64) for cb in (0, 1)]
+    del U
+    A1 = fields.random_clover(G, seed=78, device=dev)
+    A0 = fields.invert_blocks(fields.random_clover(G, seed=79, device=dev))
+    clov = [layout.pack_clover(G, A0, torch.float64), layout.pack_clover(G, A1, torch.float64)]
+    del A0, A1
+    p = dict(coeff_s=kappa, coeff_t_f=kappa, coeff_t_b=kappa, rho=0.0)
+    ops_ = {}
+    for ft, dt in ((F64, torch.float64), (F32, torch.float32), (F16, torch.float16)):
+        gg = G.with_(ftype=ft)
+        ops_[ft] = EvenOddOperator(gg, "clover", gauge=[x.to(dt) for x in gauge], clov=[x.to(dt) for x in clov],
+                                   target_cb=1, **p)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(80)
+    bs = [layout.pack_spinor(G, fields.random_spinor(G, seed=81 + i, device=dev), torch.float64)
+          for i in range(nrhs)]
+    out = {"lattice": list(dims), "nrhs": nrhs, "tol": 1e-10, "kappa": kappa, "family": "clover"}
+    # warm-up of each path on one source
+    ops_[F64].cg(bs[0], tol=1e-4, max_iter=50)
+    mixed_solve(ops_[F64], ops_[F32], bs[0], tol=1e-4, inner_tol=1e-2)
+    mrhs.mixed_solve(ops_[F64], ops_[F16], bs, tol=1e-3, inner_tol=1e-2)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, r
+
+    t64, r64 = timed(lambda: [ops_[F64].cg(b, tol=1e-10, max_iter=5000) for b in bs])
+    out["fp64_cg"] = {"seconds": t64, "iters": [r[1]["iters"] for r in r64],
+                      "max_rel_res": max(r[1]["rel_res"] for r in r64)}
+    t32, r32 = timed(lambda: [mixed_solve(ops_[F64], ops_[F32], b, tol=1e-10, inner_tol=1e-5) for b in bs])
+    out["fp32_fp64_single_rhs"] = {"seconds": t32, "inner_iters": [r[1]["inner_iters"] for r in r32],
+                                   "max_rel_res": max(r[1]["rel_res"] for r in r32)}
+    t16, r16 = timed(lambda: mrhs.mixed_solve(ops_[F64], ops_[F16], bs, tol=1e-10, inner_tol=1e-2))
+    out["fp16_multi_rhs_mixed"] = {"seconds": t16, "inner_iters": r16[1]["inner_iters"],
+                                   "outer_iters": r16[1]["outer_iters"], "max_rel_res": max(r16[1]["rel_res"])}
+    out["speedup_vs_fp32_fp64_single_rhs"] = t32 / t16
+    out["speedup_vs_fp64_cg"] = t64 / t16
+    return out
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -353,6 +442,11 @@ def b200_arm(args, world, rank, local):
             b = layout.unpack_spinor(gr, torch.from_numpy(r["out"][: gr.spinor_elems].copy()))
             cpu["max_abs_diff_vs_gpu"] = float((a - b).abs().max())
 
+    extras = {}
+    if world == 1 and not args.no_extras:
+        extras["mrhs"] = bench_mrhs(g, f, dev)
+        extras["solve"] = bench_solve(dims, dev)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": gflops, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
@@ -372,6 +466,7 @@ def b200_arm(args, world, rank, local):
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clk.summary(),
         }
+        line.update(extras)
         print(json.dumps(line))
     if world > 1:
         dist.barrier()

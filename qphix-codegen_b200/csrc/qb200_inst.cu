@@ -20,9 +20,13 @@ template <typename FT, int S, bool COMP12, int FAM, bool ACH, bool MR>
 cudaError_t go(const KArgs<FT> &a, const GeoDev &g, const OpDev<typename ftraits<FT>::C> &p,
                cudaStream_t st)
 {
-  const long long n = (long long)g.nsites * (MR ? g.nrhs : 1);
-  const int blocks = (int)((n + kThreads - 1) / kThreads);
-  site_dslash_kernel<FT, S, COMP12, FAM, ACH, MR><<<blocks, kThreads, 0, st>>>(a, g, p);
+  // one grid row per (z, t) plane
+  const long long n = (long long)g.nxh * g.ny * (MR ? g.nrhs : 1);
+  const dim3 grid((unsigned)((n + kThreads - 1) / kThreads), (unsigned)(g.nz * g.nt));
+  if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
+  // VECLEN known at compile time for the V == S layouts
+  if (S >= 4 && g.V == S) site_dslash_kernel<FT, S, COMP12, FAM, ACH, MR, (S >= 4 ? S : 0)><<<grid, kThreads, 0, st>>>(a, g, p);
+  else site_dslash_kernel<FT, S, COMP12, FAM, ACH, MR, 0><<<grid, kThreads, 0, st>>>(a, g, p);
   return cudaGetLastError();
 }
 

@@ -1,5 +1,6 @@
 // qb200_site_kernel.cuh -- thread-per-site dslash kernel, generic over every
-// QPhiX tile layout (storage type FT, SOALEN S, VECLEN as run-time V).
+// QPhiX tile layout (storage type FT, SOALEN S; VECLEN compile-time when it
+// equals S, else run-time).
 //
 // One thread computes one output site of the checkerboard: the eight hops of
 // dslash_body (codegen/dslash.cc:200-323) in registers, followed by the
@@ -19,28 +20,73 @@ template <typename FT> struct KArgs {
   elem_t<FT> *out;
 };
 
-template <typename FT, int S, bool COMP12, int D, bool MR>
+// element offset from a site's spinor base to the base of its neighbour in
+// direction D (periodic wrap inside the local lattice).  ue: elements per
+// block, le: elements per lane step (1, or nrhs in the multi-RHS layout).
+template <int S, int D>
+__device__ __forceinline__ long long neighbour_offset(const GeoDev &g, const Site &s, long long ue, int le,
+                                                      bool *cross)
+{
+  const int lane = s.xcb % S;
+  const int xb = s.xcb / S;
+  if (D == 0) {
+    *cross = (s.par == 0) && (s.xcb == 0);
+    if (s.par != 0) return 0;
+    if (lane > 0) return -le;
+    if (xb > 0) return -ue + (long long)(S - 1) * le;
+    return (long long)(g.nvecs - 1) * ue + (long long)(S - 1) * le;
+  } else if (D == 1) {
+    *cross = (s.par == 1) && (s.xcb == g.nxh - 1);
+    if (s.par != 1) return 0;
+    if (lane < S - 1) return le;
+    if (xb < g.nvecs - 1) return ue - (long long)(S - 1) * le;
+    return -(long long)(g.nvecs - 1) * ue - (long long)(S - 1) * le;
+  } else if (D == 2) {
+    *cross = s.y == 0;
+    return (s.y > 0 ? -1LL : (long long)(g.ny - 1)) * g.nvecs * ue;
+  } else if (D == 3) {
+    *cross = s.y == g.ny - 1;
+    return (s.y < g.ny - 1 ? 1LL : -(long long)(g.ny - 1)) * g.nvecs * ue;
+  } else if (D == 4) {
+    *cross = s.z == 0;
+    return (s.z > 0 ? -1LL : (long long)(g.nz - 1)) * g.Pxy * ue;
+  } else if (D == 5) {
+    *cross = s.z == g.nz - 1;
+    return (s.z < g.nz - 1 ? 1LL : -(long long)(g.nz - 1)) * g.Pxy * ue;
+  } else if (D == 6) {
+    *cross = s.t == 0;
+    return (s.t > 0 ? -1LL : (long long)(g.nt - 1)) * g.Pxyz * ue;
+  } else {
+    *cross = s.t == g.nt - 1;
+    return (s.t < g.nt - 1 ? 1LL : -(long long)(g.nt - 1)) * g.Pxyz * ue;
+  }
+}
+
+// VV: compile-time VECLEN (layouts with V == VV), or 0 for the run-time g.V
+template <int VV> __device__ __forceinline__ int vlen(const GeoDev &g) { return VV ? VV : g.V; }
+
+template <typename FT, int S, bool COMP12, int D, bool MR, int VV>
 __device__ __forceinline__ void do_hop(const KArgs<FT> &a, const GeoDev &g,
-                                       const OpDev<typename ftraits<FT>::C> &p, const Site &s,
-                                       long long gbase, int rhs,
+                                       const OpDev<typename ftraits<FT>::C> &p, const Site &s, long long obase,
+                                       long long ue, int le, long long gbase,
                                        cx<typename ftraits<FT>::C> (&acc)[4][3])
 {
   typedef typename ftraits<FT>::C C;
   constexpr int MU = D / 2;
   constexpr bool FWD = (D & 1) != 0;
   bool cross;
-  const Site n = neighbour<D>(g, s, &cross);
+  const long long nbase = obase + neighbour_offset<S, D>(g, s, ue, le, &cross);
   if (cross && !((p.acc_mask >> D) & 1u)) return;
   C beta = p.beta[D];
   if (D == 6 && s.t == 0 && p.t_edge_lo) beta *= p.tbound;
   if (D == 7 && s.t == g.nt - 1 && p.t_edge_hi) beta *= p.tbound;
 
   cx<C> psi[4][3], b[2][3], ub[2][3], G[3][3];
-  if (MR) load_spinor_rs<FT>(a.psi, spinor_base_mr<S>(g, n, rhs), S * g.nrhs, psi);
-  else load_spinor<FT, S>(a.psi, spinor_base<FT, S>(g, n), psi);
+  if (MR) load_spinor_rs<FT>(a.psi, nbase, S * g.nrhs, psi);
+  else load_spinor<FT, S>(a.psi, nbase, psi);
   const C sigma = p.isPlus ? (C)1 : (C)-1;
   project<C, D>(psi, sigma, b);
-  load_link<FT, COMP12, D>(a.gauge, gbase, g.V, G);
+  load_link<FT, COMP12, D>(a.gauge, gbase, vlen<VV>(g), G);
   mult_link<C, !FWD>(G, b, ub);
   if ((p.tbc_mask >> MU) & 1u) {
     const C pr = p.tbc[MU][0];
@@ -52,25 +98,35 @@ __device__ __forceinline__ void do_hop(const KArgs<FT> &a, const GeoDev &g,
   recons<C, MU>(ub, beta, tau, acc);
 }
 
-// MR: multi-RHS layout, one thread per (site, right-hand side) with the
-// right-hand side fastest, so the nrhs threads of a site share each link and
-// clover load
-template <typename FT, int S, bool COMP12, int FAM, bool ACH, bool MR>
+// Grid: blockIdx.y = the (z, t) plane, x covers the plane's sites (times the
+// right-hand sides).  MR: multi-RHS layout, one thread per (site, right-hand
+// side) with the right-hand side fastest, so the nrhs threads of a site share
+// each link and clover load.
+template <typename FT, int S, bool COMP12, int FAM, bool ACH, bool MR, int VV>
 __global__ void __launch_bounds__(128)
     site_dslash_kernel(const KArgs<FT> a, const GeoDev g, const OpDev<typename ftraits<FT>::C> p)
 {
   typedef typename ftraits<FT>::C C;
-  const int gi = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gi >= g.nsites * (MR ? g.nrhs : 1)) return;
-  const int i = MR ? gi / g.nrhs : gi;
-  const int rhs = MR ? gi - i * g.nrhs : 0;
-  const Site s = site_of(g, i, p.cb);
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nr = MR ? g.nrhs : 1;
+  if (q >= g.nxh * g.ny * nr) return;
+  const int sp = MR ? q / nr : q;
+  const int rhs = MR ? q - sp * nr : 0;
+  Site s;
+  s.z = blockIdx.y % g.nz;
+  s.t = blockIdx.y / g.nz;
+  s.y = sp / g.nxh;
+  s.xcb = sp - s.y * g.nxh;
+  s.par = (s.y + s.z + s.t + p.cb) & 1;
   int lane;
   const long long tile = tile_of<S>(g, s, &lane);
   constexpr int R = COMP12 ? 2 : 3;
-  const long long gbase = tile * (8LL * R * 6 * g.V) + lane;
+  const int V = vlen<VV>(g);
+  const long long gbase = tile * (8LL * R * 6 * V) + lane;
   const long long obase = MR ? spinor_base_mr<S>(g, s, rhs) : spinor_base<FT, S>(g, s);
-  const int cs = S * g.nrhs;
+  const long long ue = MR ? 24LL * S * nr : (long long)ftraits<FT>::SPB * S;
+  const int le = nr;
+  const int cs = S * nr;
 
   cx<C> res[4][3];
   cx<C> acc[4][3];
@@ -101,11 +157,11 @@ __global__ void __launch_bounds__(128)
                              p.alpha * fma(m, ch[sp][c].re, ch[sp][c].im));
       }
     } else {
-      const long long cbase = tile * ((FAM == FAM_CLOVER ? 72LL : 144LL) * g.V) + lane;
+      const long long cbase = tile * ((FAM == FAM_CLOVER ? 72LL : 144LL) * V) + lane;
 #pragma unroll
       for (int blk = 0; blk < 2; blk++) {
-        if (FAM == FAM_CLOVER) clover_block<FT, false>(a.clov, cbase, g.V, blk, ch, res);
-        else full_clover_block<FT, false>(a.clov, cbase, g.V, blk, ch, res);
+        if (FAM == FAM_CLOVER) clover_block<FT, false>(a.clov, cbase, V, blk, ch, res);
+        else full_clover_block<FT, false>(a.clov, cbase, V, blk, ch, res);
       }
       // + i rho g5 chi for plus (dslash_common.cc:1873-1906)
 #pragma unroll
@@ -118,33 +174,33 @@ __global__ void __launch_bounds__(128)
         }
       }
     }
-    do_hop<FT, S, COMP12, 0, MR>(a, g, p, s, gbase, rhs, res);
-    do_hop<FT, S, COMP12, 1, MR>(a, g, p, s, gbase, rhs, res);
-    do_hop<FT, S, COMP12, 2, MR>(a, g, p, s, gbase, rhs, res);
-    do_hop<FT, S, COMP12, 3, MR>(a, g, p, s, gbase, rhs, res);
-    do_hop<FT, S, COMP12, 4, MR>(a, g, p, s, gbase, rhs, res);
-    do_hop<FT, S, COMP12, 5, MR>(a, g, p, s, gbase, rhs, res);
-    do_hop<FT, S, COMP12, 6, MR>(a, g, p, s, gbase, rhs, res);
-    do_hop<FT, S, COMP12, 7, MR>(a, g, p, s, gbase, rhs, res);
+    do_hop<FT, S, COMP12, 0, MR, VV>(a, g, p, s, obase, ue, le, gbase, res);
+    do_hop<FT, S, COMP12, 1, MR, VV>(a, g, p, s, obase, ue, le, gbase, res);
+    do_hop<FT, S, COMP12, 2, MR, VV>(a, g, p, s, obase, ue, le, gbase, res);
+    do_hop<FT, S, COMP12, 3, MR, VV>(a, g, p, s, obase, ue, le, gbase, res);
+    do_hop<FT, S, COMP12, 4, MR, VV>(a, g, p, s, obase, ue, le, gbase, res);
+    do_hop<FT, S, COMP12, 5, MR, VV>(a, g, p, s, obase, ue, le, gbase, res);
+    do_hop<FT, S, COMP12, 6, MR, VV>(a, g, p, s, obase, ue, le, gbase, res);
+    do_hop<FT, S, COMP12, 7, MR, VV>(a, g, p, s, obase, ue, le, gbase, res);
   } else {
 #pragma unroll
     for (int sp = 0; sp < 4; sp++)
 #pragma unroll
       for (int c = 0; c < 3; c++) acc[sp][c] = mk<C>(0, 0);
-    do_hop<FT, S, COMP12, 0, MR>(a, g, p, s, gbase, rhs, acc);
-    do_hop<FT, S, COMP12, 1, MR>(a, g, p, s, gbase, rhs, acc);
-    do_hop<FT, S, COMP12, 2, MR>(a, g, p, s, gbase, rhs, acc);
-    do_hop<FT, S, COMP12, 3, MR>(a, g, p, s, gbase, rhs, acc);
-    do_hop<FT, S, COMP12, 4, MR>(a, g, p, s, gbase, rhs, acc);
-    do_hop<FT, S, COMP12, 5, MR>(a, g, p, s, gbase, rhs, acc);
-    do_hop<FT, S, COMP12, 6, MR>(a, g, p, s, gbase, rhs, acc);
-    do_hop<FT, S, COMP12, 7, MR>(a, g, p, s, gbase, rhs, acc);
+    do_hop<FT, S, COMP12, 0, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
+    do_hop<FT, S, COMP12, 1, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
+    do_hop<FT, S, COMP12, 2, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
+    do_hop<FT, S, COMP12, 3, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
+    do_hop<FT, S, COMP12, 4, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
+    do_hop<FT, S, COMP12, 5, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
+    do_hop<FT, S, COMP12, 6, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
+    do_hop<FT, S, COMP12, 7, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
     if (FAM == FAM_CLOVER || FAM == FAM_TMCLOV) {
-      const long long cbase = tile * ((FAM == FAM_CLOVER ? 72LL : 144LL) * g.V) + lane;
+      const long long cbase = tile * ((FAM == FAM_CLOVER ? 72LL : 144LL) * V) + lane;
 #pragma unroll
       for (int blk = 0; blk < 2; blk++) {
-        if (FAM == FAM_CLOVER) clover_block<FT, false>(a.clov, cbase, g.V, blk, acc, res);
-        else full_clover_block<FT, false>(a.clov, cbase, g.V, blk, acc, res);
+        if (FAM == FAM_CLOVER) clover_block<FT, false>(a.clov, cbase, V, blk, acc, res);
+        else full_clover_block<FT, false>(a.clov, cbase, V, blk, acc, res);
       }
     } else if (FAM == FAM_TM) {
       inv_twisted<C, false>(acc, p.isPlus, p.mu, p.muinv, res);
