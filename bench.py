@@ -295,6 +295,46 @@ def bench_solve(dims, dev, nrhs=8, kappa=0.16):
     return out
 
 
+def bench_force(dev, dims=(24, 24, 24, 48)):
+    """Backward of the hopping term at 24^3x48, FP32, 18-real links: the
+    link-force kernel (plain and su(3)-projected) against its algorithmic
+    bytes (chi + psi read once, 8 x 72 B written per site; + 8 x 72 B of links
+    when projecting), the forward dslash it differentiates, and one full
+    torch.autograd step (forward, dagger for the spinor cotangent, force,
+    fold onto the full-lattice links)."""
+    from qphix_b200 import autograd as AG
+    from qphix_b200 import fields, layout, ops
+    from qphix_b200.lattice import F32, Geometry
+    g = Geometry(*dims, soalen=4, ftype=F32, t_boundary=-1.0)     # nx/2 = 12 sites: SOALEN 4
+    n = g.vol_cb
+    stream = torch.cuda.current_stream()
+    U = fields.random_gauge(g, seed=90, device=dev).to(torch.complex64)
+    gauge0 = layout.pack_gauge(g, U, 0)
+    psi = layout.pack_spinor(g, fields.random_spinor(g, seed=91, device=dev))
+    chi = layout.pack_spinor(g, fields.random_spinor(g, seed=92, device=dev))
+    F = torch.empty(144 * n, dtype=torch.float32, device=dev)
+    out = torch.zeros_like(psi)
+    t_force = _time(lambda: AG.hop_force(g, 0, 1, chi, psi, out=F), 20, stream)
+    t_proj = _time(lambda: AG.hop_force(g, 0, 1, chi, psi, gauge0, out=F), 20, stream)
+    t_fwd = _time(lambda: ops.dslash(g, "wilson", "dslash", 1, 0, psi, out, gauge0), 20, stream)
+    Ur = U.clone().requires_grad_(True)
+    pr = psi.clone().requires_grad_(True)
+
+    def step():
+        Ur.grad = None
+        pr.grad = None
+        (chi * AG.WilsonHop.apply(pr, Ur, g, 0, 1, None)).sum().backward()
+
+    t_step = _time(step, 5, stream)
+    b_force, b_proj = 96 + 96 + 576, 96 + 96 + 576 + 576
+    return {"lattice": list(dims), "dtype": "f32", "sites_per_cb": n,
+            "force_ms": t_force, "force_gbs": b_force * n / (t_force * 1e-3) / 1e9, "force_bytes_per_site": b_force,
+            "projected_force_ms": t_proj, "projected_force_gbs": b_proj * n / (t_proj * 1e-3) / 1e9,
+            "projected_force_bytes_per_site": b_proj, "wilson_dslash_ms": t_fwd,
+            "autograd_step_ms": t_step,
+            "note": "autograd step = forward dslash + dagger dslash + force + torch packing/folding of links"}
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -446,6 +486,7 @@ def b200_arm(args, world, rank, local):
     if world == 1 and not args.no_extras:
         extras["mrhs"] = bench_mrhs(g, f, dev)
         extras["solve"] = bench_solve(dims, dev)
+        extras["force"] = bench_force(dev)
 
     if rank == 0:
         line = {

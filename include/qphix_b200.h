@@ -397,6 +397,11 @@ long long qb200_cg_workspace_bytes(const qb200_lattice *lat);
 long long qb200_bicgstab_workspace_bytes(const qb200_lattice *lat);
 int qb200_invert_cg(const qb200_lattice *lat, const qb200_operator *op, const void *b, void *x, double rel_tol,
                     int max_iter, void *workspace, int *iters, double *rel_res, void *stream);
+/* CG on the normal operator itself: Mhat^dag Mhat x = b (the solve a
+ * pseudofermion action or force needs); workspace of qb200_cg_workspace_bytes;
+ * rel_res = |b - Mhat^dag Mhat x| / |b| */
+int qb200_invert_cg_normal(const qb200_lattice *lat, const qb200_operator *op, const void *b, void *x,
+                           double rel_tol, int max_iter, void *workspace, int *iters, double *rel_res, void *stream);
 int qb200_invert_bicgstab(const qb200_lattice *lat, const qb200_operator *op, const void *b, void *x,
                           double rel_tol, int max_iter, void *workspace, int *iters, double *rel_res,
                           void *stream);
@@ -456,6 +461,28 @@ int qb200_invert_mixed_mrhs(const qb200_lattice *lat_hi, const qb200_operator *o
                             const qb200_operator *op_lo, int nrhs, const void *const *b, void *const *x,
                             double rel_tol, double inner_tol, int max_inner, int max_outer, void *ws_hi, void *ws_lo,
                             int *inner_iters, int *outer_iters, double *rel_res, void *stream);
+
+/* ---- backward: link derivative of the hopping term ----------------------
+ * No counterpart in the reference (it has no backward kernels).
+ *
+ * For L = Re <chi, H psi>, H the eight-hop sum of the plain Wilson dslash on
+ * checkerboard cb (qb200_dslash_plus_vec / _minus_vec by isign, same
+ * coefficients, twisted phases and time boundary; chi on cb, psi on 1 - cb),
+ * writes for each site of cb and each of its eight stored links U
+ * (direction 2*mu+1: U_mu(x); 2*mu: U_mu(x - mu)):
+ *   gauge == NULL:  F = dL/dRe U + i dL/dIm U                  (3 x 3 complex)
+ *   gauge != NULL:  P = TA(F U^dag), the traceless anti-Hermitian
+ *                   projection, using the links of `gauge` (checkerboard cb,
+ *                   18 or 12 reals); dL/deps along U -> exp(eps X) U is
+ *                   Re tr(X^dag P).
+ * Layout: real component k = ((dir*3 + row)*3 + col)*2 + re/im of the i-th
+ * site of cb in (t, z, y, xcb) order at force[k * nsites + i]
+ * (qb200_hop_force_elems reals).  FP32 or FP64 storage; the spinor
+ * cotangent of L is the dagger dslash (isign flipped) of chi. */
+long long qb200_hop_force_elems(const qb200_lattice *lat);
+int qb200_hop_force(const qb200_lattice *lat, int cb, int isign, const void *chi, const void *psi,
+                    const void *gauge, double coeff_s, double coeff_t_f, double coeff_t_b, unsigned tbc_mask,
+                    const double *tbc_phases, void *force, void *stream);
 
 #ifdef __cplusplus
 }

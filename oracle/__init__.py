@@ -114,6 +114,7 @@ def liboracle():
         L.oracle_face_count.restype = ctypes.c_longlong
         L.oracle_face_pack.argtypes = [LP, I, I, V, V, I, V]
         L.oracle_face_unpack.argtypes = [LP, I, I, I, V, V, V, V, D, D, D, I, I, V, V]
+        L.oracle_hop_force.argtypes = [LP, I, I, V, V, V, ctypes.POINTER(Params), V]
         _oracle = L
     return _oracle
 
@@ -159,6 +160,22 @@ def face_unpack(g, family, isign, cb, inbuf, gauge, out, dir, beta=1.0, clover=N
                               _ptr(ph), _ptr(scratch))
     if rc:
         raise RuntimeError("oracle_face_unpack failed: %d" % rc)
+    return out
+
+
+def hop_force(g, isign, cb, chi, psi, gauge=None, params=None):
+    """FP64 link derivative of Re <chi, H psi> (H: plain Wilson hopping term on
+    cb), or its su(3) projection when `gauge` (checkerboard cb) is given.
+    Returns a float64 array of 144 * (sites of cb) reals laid out as
+    qb200_hop_force's output."""
+    L = liboracle()
+    lat = lattice_struct(g)
+    p = params if params is not None else make_params()
+    out = np.zeros(144 * g.nx // 2 * g.ny * g.nz * g.nt, dtype=np.float64)
+    rc = L.oracle_hop_force(ctypes.byref(lat), 1 if isign > 0 else -1, cb, _ptr(chi), _ptr(psi), _ptr(gauge),
+                            ctypes.byref(p), _ptr(out))
+    if rc:
+        raise RuntimeError("oracle_hop_force failed: %d" % rc)
     return out
 
 

@@ -476,6 +476,96 @@ int oracle_dslash(const qb200_lattice *lat, int family, int achimbdpsi,
 }
 
 /* ------------------------------------------------------------------ */
+/* link derivative of the hopping term (no counterpart in the reference)  */
+
+/* Re <chi, beta recons(tbc(mult_link(G, b)))> of one hop, for a given G:
+ * the same steps as the hop loop of oracle_dslash (dslash_common.cc:
+ * 1729-1826).  The derivative with respect to the link is taken below by
+ * linearity: the hop is linear in G (forward) or in conj(G) (backward), so
+ * evaluating it on the unit matrices gives dL/dRe G and dL/dIm G exactly. */
+static double hop_value(int d, int isPlus, double beta, const oracle_params *p,
+                        cplx G[3][3], cplx b[2][3], cplx ch[4][3])
+{
+  int mu = d / 2, fwd = d & 1;
+  cplx ub[2][3], hop[4][3];
+  memset(hop, 0, sizeof(hop));
+  mult_link(G, !fwd, b, ub);
+  if (p->tbc_mask & (1u << mu)) apply_tbc(fwd, p->tbc_phases[mu], ub);
+  recons(mu, isPlus ? !fwd : fwd, beta, ub, hop);
+  double v = 0;
+  for (int s = 0; s < 4; s++)
+    for (int c = 0; c < 3; c++) v += creal(conj(ch[s][c]) * hop[s][c]);
+  return v;
+}
+
+/* force[((d*3+r)*3+c)*2+ri][i] = dL/dU (gauge == NULL) or TA(dL/dU U^dag)
+ * for L = Re <chi, H psi>, H the plain Wilson hopping term on cb; see
+ * qb200_hop_force in include/qphix_b200.h.  FP64 output. */
+int oracle_hop_force(const qb200_lattice *lat, int isign, int cb, const void *chi,
+                     const void *psi, const void *gauge, const oracle_params *p,
+                     double *force)
+{
+  geo g;
+  if (make_geo(lat, &g)) return QB200_EINVAL;
+  if (!chi || !psi || !force) return QB200_ENULL;
+  int isPlus = isign > 0;
+  long long nsites = (long long)g.nxh * g.ny * g.nz * g.nt;
+
+#pragma omp parallel for schedule(static)
+  for (long long i = 0; i < nsites; i++) {
+    int xcb = (int)(i % g.nxh);
+    long long r = i / g.nxh;
+    int y = (int)(r % g.ny); r /= g.ny;
+    int z = (int)(r % g.nz);
+    int t = (int)(r / g.nz);
+    cplx ch[4][3];
+    load_spinor(&g, chi, xcb, y, z, t, ch);
+    for (int d = 0; d < 8; d++) {
+      int mu = d / 2, fwd = d & 1;
+      int ax, ay, az, at;
+      neighbour(&g, cb, d, xcb, y, z, t, &ax, &ay, &az, &at);
+      double beta = mu < 3 ? p->coeff_s : (fwd ? p->coeff_t_f : p->coeff_t_b);
+      if (mu == 3 && fwd && t == g.nt - 1 && lat->t_edge_hi) beta *= lat->t_boundary;
+      if (mu == 3 && !fwd && t == 0 && lat->t_edge_lo) beta *= lat->t_boundary;
+      cplx nb[4][3], b[2][3];
+      load_spinor(&g, psi, ax, ay, az, at, nb);
+      project(isPlus ? d : (d ^ 1), nb, b);
+      /* F_U[c][r] = dL/dRe G[r][c] + i dL/dIm G[r][c]  (U = G^T) */
+      cplx F[3][3];
+      for (int rr = 0; rr < 3; rr++)
+        for (int cc = 0; cc < 3; cc++) {
+          cplx E[3][3];
+          memset(E, 0, sizeof(E));
+          E[rr][cc] = 1.0;
+          double dre = hop_value(d, isPlus, beta, p, E, b, ch);
+          E[rr][cc] = I;
+          double dim = hop_value(d, isPlus, beta, p, E, b, ch);
+          F[cc][rr] = dre + I * dim;
+        }
+      if (gauge) {
+        cplx G[3][3], M[3][3];
+        load_link(&g, gauge, xcb, y, z, t, d, G);
+        for (int a = 0; a < 3; a++)
+          for (int c = 0; c < 3; c++) {
+            cplx acc = 0;
+            for (int k = 0; k < 3; k++) acc += F[a][k] * conj(G[k][c]); /* U^dag[k][c] = conj(G[k][c]) */
+            M[a][c] = acc;
+          }
+        cplx tr = (M[0][0] - conj(M[0][0]) + M[1][1] - conj(M[1][1]) + M[2][2] - conj(M[2][2])) / 6.0;
+        for (int a = 0; a < 3; a++)
+          for (int c = 0; c < 3; c++) F[a][c] = 0.5 * (M[a][c] - conj(M[c][a])) - (a == c ? tr : 0.0);
+      }
+      for (int a = 0; a < 3; a++)
+        for (int c = 0; c < 3; c++) {
+          force[((long long)((d * 3 + a) * 3 + c) * 2 + 0) * nsites + i] = creal(F[a][c]);
+          force[((long long)((d * 3 + a) * 3 + c) * 2 + 1) * nsites + i] = cimag(F[a][c]);
+        }
+    }
+  }
+  return QB200_OK;
+}
+
+/* ------------------------------------------------------------------ */
 /* faces                                                                */
 
 /* enumerate the sites of checkerboard cb whose coordinate in dim mu is

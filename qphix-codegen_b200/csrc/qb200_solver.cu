@@ -562,6 +562,23 @@ int true_residual(const qb200_lattice *l, const qb200_operator *op, const void *
   return QB200_OK;
 }
 
+// |b - Mhat^dag Mhat x| / |b|; r, t, tmp: scratch spinors
+int true_residual_normal(const qb200_lattice *l, const qb200_operator *op, const void *b, const void *x, void *r,
+                         void *t, void *tmp, double *partials, double *scal, double *rel, cudaStream_t st)
+{
+  const VS V = vs_of(l);
+  int rc = normal_op(l, op, x, r, t, tmp, st);
+  if (rc) return rc;
+  cudaError_t e = axpby(V, host(1.0), b, host(-1.0), r, st);
+  if (e == cudaSuccess) e = dot(V, r, r, partials, scal, st);
+  if (e == cudaSuccess) e = dot(V, b, b, partials, scal + 1, st);
+  if ((rc = cuda_rc(e, "true residual"))) return rc;
+  double h[2];
+  if ((rc = fetch(h, scal, 2, st))) return rc;
+  *rel = h[1] > 0 ? std::sqrt(h[0] / h[1]) : 0.0;
+  return QB200_OK;
+}
+
 bool same_shape(const qb200_lattice *a, const qb200_lattice *b)
 {
   return a->nx == b->nx && a->ny == b->ny && a->nz == b->nz && a->nt == b->nt && a->soalen == b->soalen &&
@@ -716,6 +733,25 @@ int qb200_invert_cg(const qb200_lattice *lat, const qb200_operator *op, const vo
   if (iters) *iters = k;
   double tr = 0.0;
   if ((rc = true_residual(lat, op, b, x, s.v[0], s.v[4], s.partials, s.scal + 10, &tr, st))) return rc;
+  if (rel_res) *rel_res = tr;
+  return QB200_OK;
+}
+
+int qb200_invert_cg_normal(const qb200_lattice *lat, const qb200_operator *op, const void *b, void *x,
+                           double rel_tol, int max_iter, void *workspace, int *iters, double *rel_res, void *stream)
+{
+  int rc = check_op(lat, op);
+  if (rc) return rc;
+  if (!b || !x || !workspace) return api_fail(QB200_ENULL, "b, x and workspace must be non-NULL");
+  cudaStream_t st = (cudaStream_t)stream;
+  Vecs s = carve(lat, workspace, 6);
+  int k = 0;
+  double rel = 0.0;
+  if ((rc = cg_core(lat, op, b, x, rel_tol, max_iter, s, &k, &rel, st))) return rc;
+  if (iters) *iters = k;
+  double tr = 0.0;
+  if ((rc = true_residual_normal(lat, op, b, x, s.v[0], s.v[3], s.v[4], s.partials, s.scal + 10, &tr, st)))
+    return rc;
   if (rel_res) *rel_res = tr;
   return QB200_OK;
 }

@@ -87,6 +87,7 @@ SIGNATURES.update({
     "qb200_blas_cdot": [_LAT, _P, _P, _P, _P, _P],
     "qb200_invert_cg": [_LAT, _OP, _P, _P, _D, _I, _P, _IP, _DP, _P],
     "qb200_invert_bicgstab": [_LAT, _OP, _P, _P, _D, _I, _P, _IP, _DP, _P],
+    "qb200_invert_cg_normal": [_LAT, _OP, _P, _P, _D, _I, _P, _IP, _DP, _P],
     "qb200_invert_mixed": [_LAT, _OP, _LAT, _OP, _I, _P, _P, _D, _D, _I, _I, _P, _P, _IP, _IP, _DP, _P],
 })
 INFO.update({
@@ -121,6 +122,12 @@ INFO.update({
     "qb200_mrhs_spinor_elems": ([_LAT, _I], _LL),
     "qb200_cg_mrhs_workspace_bytes": ([_LAT, _I], _LL),
     "qb200_mixed_mrhs_workspace_bytes": ([_LAT, _LAT, _I, ctypes.POINTER(_LL)], _LL),
+})
+SIGNATURES.update({
+    "qb200_hop_force": [_LAT, _I, _I, _P, _P, _P, _D, _D, _D, _U, _DA, _P, _P],
+})
+INFO.update({
+    "qb200_hop_force_elems": ([_LAT], _LL),
 })
 
 _lib = None

@@ -79,6 +79,10 @@ class EvenOddOperator:
         """CG on Mhat^dag Mhat x = Mhat^dag b (x: initial guess, default 0)."""
         return self._solve("qb200_invert_cg", "qb200_cg_workspace_bytes", b, x, tol, max_iter)
 
+    def cg_normal(self, b, x=None, tol=1e-10, max_iter=10000):
+        """CG on Mhat^dag Mhat x = b (rel_res: |b - Mhat^dag Mhat x| / |b|)."""
+        return self._solve("qb200_invert_cg_normal", "qb200_cg_workspace_bytes", b, x, tol, max_iter)
+
     def bicgstab(self, b, x=None, tol=1e-10, max_iter=10000):
         return self._solve("qb200_invert_bicgstab", "qb200_bicgstab_workspace_bytes", b, x, tol, max_iter)
 

@@ -149,3 +149,24 @@ def oracle_schur(g: Geometry, family, f, p, x, isign=1, target_cb=1):
     p2 = O.make_params(**q)
     return O.dslash(g, family, "achimbdpsi", isign, target_cb, tmp, f["gauge"][target_cb], chi=x,
                     clover=clov[target_cb], params=p2)
+
+
+def random_algebra(shape, seed):
+    """Gaussian traceless anti-Hermitian 3x3 matrices (an su(3) direction per link)."""
+    gen = torch.Generator().manual_seed(seed)
+    m = torch.complex(torch.randn(tuple(shape) + (3, 3), generator=gen, dtype=torch.float64),
+                      torch.randn(tuple(shape) + (3, 3), generator=gen, dtype=torch.float64))
+    a = 0.5 * (m - m.conj().transpose(-1, -2))
+    tr = torch.diagonal(a, dim1=-2, dim2=-1).sum(-1) / 3.0
+    return a - tr[..., None, None] * torch.eye(3, dtype=a.dtype)
+
+
+def moved_links(U, X, eps):
+    """exp(eps X) U, link by link."""
+    return torch.linalg.matrix_exp(eps * X.to(U.device)) @ U
+
+
+def directional(gU, X, U):
+    """sum Re <gU, X U>: the derivative along U -> exp(eps X) U of a loss whose
+    link gradient (torch convention) is gU."""
+    return float((gU.conj() * (X.to(U.device) @ U)).real.sum())
