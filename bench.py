@@ -222,21 +222,28 @@ def _time(fn, reps, stream):
 
 def bench_mrhs(g, f, dev):
     """Multi-RHS clover A.chi - b.D.psi: nrhs right-hand sides share one link
-    and clover field; per right-hand-side site 288 + 672/nrhs bytes."""
+    and clover field; per right-hand-side site 3 spinors + (links + clover) /
+    nrhs bytes: FP32 288 + 672/nrhs, FP16 144 + 336/nrhs."""
     from qphix_b200 import mrhs
+    from qphix_b200.lattice import F16
     res = {}
     stream = torch.cuda.current_stream()
-    for n in (4, 8, 16):
-        psi = torch.randn(g.spinor_elems * n, device=dev)
-        chi = torch.randn(g.spinor_elems * n, device=dev)
-        out = torch.zeros_like(psi)
-        ms = _time(lambda: mrhs.dslash(g, n, "clover", "achimbdpsi", 1, 0, psi, out, f["gauge"], chi=chi,
-                                       clover=f["clover"], **PARAMS), 20, stream)
-        bps = 3 * 96 + (384 + 288) / n
-        res["nrhs_%d" % n] = {"ms_per_call": ms, "gflops": FLOP_SITE * g.vol_cb * n / (ms * 1e-3) / 1e9,
-                              "gbs": bps * g.vol_cb * n / (ms * 1e-3) / 1e9, "bytes_per_rhs_site": bps}
-        del psi, chi, out
-    res["note"] = "GB/s against 288 + 672/nrhs algorithmic bytes per right-hand-side site"
+    g16 = g.with_(ftype=F16)
+    fields16 = {"gauge": f["gauge"].half(), "clover": f["clover"].half()}
+    for tag, gg, ff, sp_b, lc_b in (("f32", g, f, 96, 672), ("f16", g16, fields16, 48, 336)):
+        for n in (4, 8, 16):
+            psi = torch.randn(gg.spinor_elems * n, device=dev).to(gg.dtype)
+            chi = torch.randn(gg.spinor_elems * n, device=dev).to(gg.dtype)
+            out = torch.zeros_like(psi)
+            ms = _time(lambda: mrhs.dslash(gg, n, "clover", "achimbdpsi", 1, 0, psi, out, ff["gauge"], chi=chi,
+                                           clover=ff["clover"], **PARAMS), 20, stream)
+            bps = 3 * sp_b + lc_b / n
+            res["%s_nrhs_%d" % (tag, n)] = {"ms_per_call": ms,
+                                            "gflops": FLOP_SITE * g.vol_cb * n / (ms * 1e-3) / 1e9,
+                                            "gbs": bps * g.vol_cb * n / (ms * 1e-3) / 1e9, "bytes_per_rhs_site": bps}
+            del psi, chi, out
+    res["note"] = ("two right-hand sides per thread in packed FP32x2 arithmetic; GB/s against the algorithmic "
+                   "bytes per right-hand-side site")
     return res
 
 

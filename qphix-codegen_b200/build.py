@@ -58,6 +58,11 @@ def newest_source():
                for d in (CSRC, INCLUDE) for f in os.listdir(d))
 
 
+def newest_header():
+    return max(os.path.getmtime(os.path.join(d, f))
+               for d in (CSRC, INCLUDE) for f in os.listdir(d) if not f.endswith(".cu"))
+
+
 def compile_one(obj, extra, src, log):
     cmd = [nvcc()] + ARCH + NVFLAGS + extra + ["-c", src, "-o", obj]
     r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
@@ -75,8 +80,11 @@ def build(jobs=None, force=False, verbose=True):
         return LIB
     jobs = jobs or max(1, os.cpu_count() or 1)
     todo = []
+    hdr_t = newest_header()
     for obj, extra, src in units():
-        if force or not os.path.exists(obj) or os.path.getmtime(obj) < src_t:
+        # a unit depends on its own source and on every header
+        dep_t = max(hdr_t, os.path.getmtime(src))
+        if force or not os.path.exists(obj) or os.path.getmtime(obj) < dep_t:
             todo.append((obj, extra, src, obj + ".log"))
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
         futs = [ex.submit(compile_one, *t) for t in todo]

@@ -382,8 +382,9 @@ __device__ __forceinline__ void apply_phase(cx<C> (&ub)[2][3], C pr, C pi)
   for (int s = 0; s < 2; s++)
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      const C re = pr * ub[s][c].re - pi * ub[s][c].im;
-      const C im = pr * ub[s][c].im + pi * ub[s][c].re;
+      // explicit contraction order (the multi-RHS pair kernel repeats it)
+      const C re = fma(-pi, ub[s][c].im, pr * ub[s][c].re);
+      const C im = fma(pi, ub[s][c].re, pr * ub[s][c].im);
       ub[s][c].re = re;
       ub[s][c].im = im;
     }

@@ -3,6 +3,9 @@
 // translation units build in parallel.
 #include "qb200_face_kernel.cuh"
 #include "qb200_internal.h"
+#if QB_MRHS
+#include "qb200_pair_kernel.cuh"
+#endif
 
 #ifndef QB_FT
 #error "QB_FT (float, double, __half) must be defined"
@@ -46,6 +49,37 @@ cudaError_t go_fam(const LaunchSpec &ls, const KArgs<FT> &a, const GeoDev &g,
   }
   return cudaErrorInvalidValue;
 }
+
+#if QB_MRHS
+// two right-hand sides per thread (even nrhs)
+template <typename FT, int S, bool COMP12, int FAM, bool ACH>
+cudaError_t go_pair(const KArgs<FT> &a, const GeoDev &g, const OpDev<float> &p, cudaStream_t st)
+{
+  const long long n = (long long)g.nxh * g.ny * (g.nrhs / 2);
+  const dim3 grid((unsigned)((n + kThreads - 1) / kThreads), (unsigned)(g.nz * g.nt));
+  if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
+  if (g.V == S) pair_dslash_kernel<FT, S, COMP12, FAM, ACH, S><<<grid, kThreads, 0, st>>>(a, g, p);
+  else pair_dslash_kernel<FT, S, COMP12, FAM, ACH, 0><<<grid, kThreads, 0, st>>>(a, g, p);
+  return cudaGetLastError();
+}
+
+template <typename FT, int S, bool COMP12>
+cudaError_t go_pair_fam(const LaunchSpec &ls, const KArgs<FT> &a, const GeoDev &g, const OpDev<float> &p,
+                        cudaStream_t st)
+{
+  switch (ls.fam * 2 + (ls.ach ? 1 : 0)) {
+  case 0: return go_pair<FT, S, COMP12, FAM_WILSON, false>(a, g, p, st);
+  case 1: return go_pair<FT, S, COMP12, FAM_WILSON, true>(a, g, p, st);
+  case 2: return go_pair<FT, S, COMP12, FAM_CLOVER, false>(a, g, p, st);
+  case 3: return go_pair<FT, S, COMP12, FAM_CLOVER, true>(a, g, p, st);
+  case 4: return go_pair<FT, S, COMP12, FAM_TM, false>(a, g, p, st);
+  case 5: return go_pair<FT, S, COMP12, FAM_TM, true>(a, g, p, st);
+  case 6: return go_pair<FT, S, COMP12, FAM_TMCLOV, false>(a, g, p, st);
+  case 7: return go_pair<FT, S, COMP12, FAM_TMCLOV, true>(a, g, p, st);
+  }
+  return cudaErrorInvalidValue;
+}
+#endif
 
 template <typename FT, int S, bool COMP12, int FAM>
 cudaError_t go_unpack(const elem_t<FT> *buf, const elem_t<FT> *gauge, const elem_t<FT> *clov, elem_t<FT> *out,
@@ -97,6 +131,8 @@ cudaError_t launch_dslash_mrhs(const LaunchSpec &ls, const elem_t<FT> *psi, cons
   a.clov = clov;
   a.out = out;
   if (g.nsites == 0) return cudaSuccess;
+  if (g.nrhs % 2 == 0)
+    return ls.comp12 ? go_pair_fam<FT, S, true>(ls, a, g, p, st) : go_pair_fam<FT, S, false>(ls, a, g, p, st);
   return ls.comp12 ? go_fam<FT, S, true, true>(ls, a, g, p, st) : go_fam<FT, S, false, true>(ls, a, g, p, st);
 }
 #endif

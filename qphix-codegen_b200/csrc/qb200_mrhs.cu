@@ -196,6 +196,26 @@ __global__ void __launch_bounds__(256) mr_slot_kernel(long long n1, int nrhs, in
   }
 }
 
+// y[j] += scale * slot of a multi-RHS array (FP64 single-layout y)
+template <typename FI>
+__global__ void __launch_bounds__(256) mr_slot_add_kernel(long long n1, int nrhs, int slot, const FI *__restrict__ in,
+                                                          double scale, double *__restrict__ y)
+{
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n1;
+       j += (long long)gridDim.x * blockDim.x)
+    y[j] += scale * to_d(in[j * nrhs + slot]);
+}
+
+cudaError_t mr_slot_add(int ft_mr, long long n1, int nrhs, int slot, const void *in, double scale, void *y,
+                        cudaStream_t st)
+{
+  const int gr = grid_for(n1);
+  if (ft_mr == QB200_F32)
+    mr_slot_add_kernel<float><<<gr, 256, 0, st>>>(n1, nrhs, slot, (const float *)in, scale, (double *)y);
+  else mr_slot_add_kernel<__half><<<gr, 256, 0, st>>>(n1, nrhs, slot, (const __half *)in, scale, (double *)y);
+  return cudaGetLastError();
+}
+
 // FP64 single field -> slot of an FP32/FP16 multi-RHS array (TO_MR), or back
 cudaError_t mr_slot(bool to_mr, int ft_mr, long long n1, int nrhs, int slot, const void *in, double scale, void *out,
                     cudaStream_t st)
@@ -226,37 +246,96 @@ struct VecScalar {
   }
 };
 
+// Element-wise and reduction kernels stream 16-byte vectors (vec16<FT>::n
+// elements).  The right-hand side of element e is e % nrhs; the grid stride,
+// a multiple of 256 vectors, is a multiple of nrhs (<= 16) elements, so each
+// lane k of a thread's vectors stays on one right-hand side.  Arithmetic is
+// FP32 for FP16 / FP32 storage and FP64 for FP64 storage; reductions
+// accumulate in FP64.
+template <typename FT> struct mr_calc {
+  typedef float T;
+};
+template <> struct mr_calc<double> {
+  typedef double T;
+};
+template <typename FT> __device__ __forceinline__ typename mr_calc<FT>::T mr_ld(FT v)
+{
+  return (typename mr_calc<FT>::T)to_d(v);
+}
+template <> __device__ __forceinline__ float mr_ld<__half>(__half v) { return __half2float(v); }
+template <> __device__ __forceinline__ float mr_ld<float>(float v) { return v; }
+template <typename FT> __device__ __forceinline__ FT mr_st(typename mr_calc<FT>::T v) { return from_d<FT>(v); }
+template <> __device__ __forceinline__ __half mr_st<__half>(float v) { return __float2half_rn(v); }
+template <> __device__ __forceinline__ float mr_st<float>(float v) { return v; }
+
 template <typename FT>
-__global__ void __launch_bounds__(256) mr_axpby_kernel(long long n, int nrhs, VecScalar a, const FT *__restrict__ x,
+__global__ void __launch_bounds__(256) mr_axpby_kernel(long long nv, int nrhs, VecScalar a, const FT *__restrict__ x,
                                                        VecScalar b, FT *__restrict__ y)
 {
-  const long long stride = (long long)gridDim.x * blockDim.x; // a multiple of nrhs
-  const long long e0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const int r = (int)(e0 % nrhs);
-  const double av = a.get(r), bv = b.get(r);
-  for (long long e = e0; e < n; e += stride) y[e] = from_d<FT>(av * to_d(x[e]) + bv * to_d(y[e]));
+  typedef typename mr_calc<FT>::T T;
+  constexpr int W = vec16<FT>::n;
+  const long long i0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  T av[W], bv[W];
+#pragma unroll
+  for (int k = 0; k < W; k++) {
+    const int r = (int)((i0 * W + k) % nrhs);
+    av[k] = (T)a.get(r);
+    bv[k] = (T)b.get(r);
+  }
+  for (long long i = i0; i < nv; i += (long long)gridDim.x * blockDim.x) {
+    const V16<FT> vx = ld16(x + i * W);
+    V16<FT> vy = ld16(y + i * W);
+#pragma unroll
+    for (int k = 0; k < W; k++) vy.e[k] = mr_st<FT>(av[k] * mr_ld(vx.e[k]) + bv[k] * mr_ld(vy.e[k]));
+    st16(y + i * W, vy);
+  }
+}
+
+// x[i] * y[i] in FP64 (FP16 products are exact in FP32)
+template <typename FT> __device__ __forceinline__ double mr_prod(FT a, FT b) { return to_d(a) * to_d(b); }
+template <> __device__ __forceinline__ double mr_prod<__half>(__half a, __half b)
+{
+  return (double)(__half2float(a) * __half2float(b));
 }
 
 // partials[r*kRedBlocks + block] = sum over the block's elements of rhs r
 template <typename FT>
-__global__ void __launch_bounds__(kRedThreads) mr_dot_kernel(long long n, int nrhs, const FT *__restrict__ x,
+__global__ void __launch_bounds__(kRedThreads) mr_dot_kernel(long long nv, int nrhs, const FT *__restrict__ x,
                                                              const FT *__restrict__ y, double *__restrict__ partials)
 {
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  const long long e0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  double s = 0.0;
-  for (long long e = e0; e < n; e += stride) s += to_d(x[e]) * to_d(y[e]);
-  // lanes with equal lane % nrhs hold the same right-hand side
-  for (int o = 16; o >= nrhs; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  __shared__ double sh[kRedThreads / 32][kMaxRhs];
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l < nrhs) sh[w][l] = s;
-  __syncthreads();
-  if (threadIdx.x < nrhs) {
-    double t = 0.0;
-    for (int i = 0; i < (int)(blockDim.x >> 5); i++) t += sh[i][threadIdx.x];
-    partials[threadIdx.x * kRedBlocks + blockIdx.x] = t;
+  constexpr int W = vec16<FT>::n;
+  __shared__ double sh[kMaxRhs];
+  if (threadIdx.x < kMaxRhs) sh[threadIdx.x] = 0.0;
+  const long long i0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double acc[W];
+#pragma unroll
+  for (int k = 0; k < W; k++) acc[k] = 0.0;
+  for (long long i = i0; i < nv; i += (long long)gridDim.x * blockDim.x) {
+    const V16<FT> vx = ld16(x + i * W);
+    const V16<FT> vy = ld16(y + i * W);
+#pragma unroll
+    for (int k = 0; k < W; k++) acc[k] += mr_prod(vx.e[k], vy.e[k]);
   }
+  __syncthreads();
+  // Lane k of warp lane l holds element offset l*W + k (mod 32*W), i.e. right-
+  // hand side (l*W + k) % nrhs.  Lanes l and l^o agree when o*W is a multiple
+  // of nrhs, so a butterfly over those o sums each right-hand side's lanes;
+  // the lanes below `first` then hold one sum per right-hand side.
+  int first = 16;
+  for (int o = 1; o <= 16; o <<= 1)
+    if (o * W >= nrhs) {
+      first = o;
+      break;
+    }
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < W; k++) {
+    double v = acc[k];
+    for (int o = 16; o >= first; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane < first) atomicAdd(&sh[(int)((i0 * W + k) % nrhs)], v);
+  }
+  __syncthreads();
+  if (threadIdx.x < nrhs) partials[threadIdx.x * kRedBlocks + blockIdx.x] = sh[threadIdx.x];
 }
 
 __global__ void mr_finish_kernel(const double *__restrict__ partials, int nrhs, double *__restrict__ result)
@@ -296,22 +375,24 @@ cudaError_t mr_axpby(const MR &m, VecScalar a, const void *x, VecScalar b, void 
 {
   // a grid stride that is a multiple of nrhs keeps each thread on one rhs
   const int blocks = 148 * 4;
-  if (m.ft == QB200_F32) mr_axpby_kernel<float><<<blocks, 256, 0, st>>>(m.n, m.nrhs, a, (const float *)x, b, (float *)y);
+  if (m.ft == QB200_F32)
+    mr_axpby_kernel<float><<<blocks, 256, 0, st>>>(m.n / 4, m.nrhs, a, (const float *)x, b, (float *)y);
   else if (m.ft == QB200_F64)
-    mr_axpby_kernel<double><<<blocks, 256, 0, st>>>(m.n, m.nrhs, a, (const double *)x, b, (double *)y);
-  else mr_axpby_kernel<__half><<<blocks, 256, 0, st>>>(m.n, m.nrhs, a, (const __half *)x, b, (__half *)y);
+    mr_axpby_kernel<double><<<blocks, 256, 0, st>>>(m.n / 2, m.nrhs, a, (const double *)x, b, (double *)y);
+  else mr_axpby_kernel<__half><<<blocks, 256, 0, st>>>(m.n / 8, m.nrhs, a, (const __half *)x, b, (__half *)y);
   return cudaGetLastError();
 }
 
 cudaError_t mr_dot(const MR &m, const void *x, const void *y, double *partials, double *result, cudaStream_t st)
 {
   if (m.ft == QB200_F32)
-    mr_dot_kernel<float><<<kRedBlocks, kRedThreads, 0, st>>>(m.n, m.nrhs, (const float *)x, (const float *)y, partials);
+    mr_dot_kernel<float><<<kRedBlocks, kRedThreads, 0, st>>>(m.n / 4, m.nrhs, (const float *)x, (const float *)y,
+                                                              partials);
   else if (m.ft == QB200_F64)
-    mr_dot_kernel<double><<<kRedBlocks, kRedThreads, 0, st>>>(m.n, m.nrhs, (const double *)x, (const double *)y,
+    mr_dot_kernel<double><<<kRedBlocks, kRedThreads, 0, st>>>(m.n / 2, m.nrhs, (const double *)x, (const double *)y,
                                                                partials);
   else
-    mr_dot_kernel<__half><<<kRedBlocks, kRedThreads, 0, st>>>(m.n, m.nrhs, (const __half *)x, (const __half *)y,
+    mr_dot_kernel<__half><<<kRedBlocks, kRedThreads, 0, st>>>(m.n / 8, m.nrhs, (const __half *)x, (const __half *)y,
                                                                partials);
   mr_finish_kernel<<<m.nrhs, kRedThreads, 0, st>>>(partials, m.nrhs, result);
   return cudaGetLastError();
@@ -542,15 +623,16 @@ long long qb200_mixed_mrhs_workspace_bytes(const qb200_lattice *lat_hi, const qb
                                            long long *lo_bytes)
 {
   if (lo_bytes) *lo_bytes = (long long)ws_bytes(lat_lo, nrhs, 8);
-  return (long long)ws_bytes(lat_hi, 1, 4);
+  return (long long)ws_bytes(lat_hi, 1, 2);
 }
 
 // Defect correction for nrhs systems: per right-hand side the true residual
-// b_i - Mhat x_i is formed with the single-RHS FP64 operator (op_hi), the
-// normal-equation residuals are packed, scaled to O(1), into one multi-RHS
-// array of the low precision, solved together with the multi-RHS low
-// precision operator (op_lo, FP16 or FP32 storage) to inner_tol, and the
-// corrections are accumulated in FP64.  b and x: host arrays of nrhs device
+// b_i - Mhat x_i is formed with the single-RHS FP64 operator (op_hi) and
+// packed, scaled to unit rms, into one multi-RHS array of the low precision;
+// the normal equations Mhat^dag Mhat e = Mhat^dag r of all right-hand sides
+// are solved together with the multi-RHS low precision operator (op_lo, FP16
+// or FP32 storage) to inner_tol, and the corrections are accumulated into x
+// in FP64.  b and x: host arrays of nrhs device
 // pointers to FP64 single-layout spinors.
 int qb200_invert_mixed_mrhs(const qb200_lattice *lat_hi, const qb200_operator *op_hi, const qb200_lattice *lat_lo,
                             const qb200_operator *op_lo, int nrhs, const void *const *b, void *const *x,
@@ -567,7 +649,7 @@ int qb200_invert_mixed_mrhs(const qb200_lattice *lat_hi, const qb200_operator *o
   cudaStream_t st = (cudaStream_t)stream;
   const long long n1 = qb200_spinor_elems(lat_hi);
   Work wh{(char *)ws_hi, 0};
-  void *r = wh.take(n1 * 8), *rn = wh.take(n1 * 8), *ehi = wh.take(n1 * 8), *tmp = wh.take(n1 * 8);
+  void *r = wh.take(n1 * 8), *tmp = wh.take(n1 * 8);
   double *partials = (double *)wh.take((size_t)kRedBlocks * 2 * 8);
   double *scal = (double *)wh.take(64 * 8);
   MRVecs L = mr_carve(lat_lo, nrhs, ws_lo, 8);
@@ -580,11 +662,13 @@ int qb200_invert_mixed_mrhs(const qb200_lattice *lat_hi, const qb200_operator *o
     if ((rc = qb200_blas_dot(QB200_F64, n1, b[i], b[i], scal, partials, st))) return rc;
     if ((rc = fetch(&bnorm[i], scal, 1, st))) return rc;
   }
+  // r_lo: the scaled true residuals in the low precision; rhs_lo = Mhat^dag r_lo
+  void *r_lo = L.v[5];
   int tot = 0, outer = 0;
   while (true) {
     bool all = true;
     for (int i = 0; i < nrhs; i++) {
-      // r = b_i - Mhat x_i ; rn = Mhat^dag r
+      // r = b_i - Mhat x_i in FP64
       if ((rc = qb200_schur_apply(lat_hi, op_hi, 1, x[i], r, tmp, st))) return rc;
       if ((rc = qb200_blas_axpby(QB200_F64, n1, 1.0, b[i], -1.0, r, st))) return rc;
       double rr;
@@ -592,29 +676,24 @@ int qb200_invert_mixed_mrhs(const qb200_lattice *lat_hi, const qb200_operator *o
       if ((rc = fetch(&rr, scal, 1, st))) return rc;
       rel[i] = bnorm[i] > 0 ? std::sqrt(rr / bnorm[i]) : 0.0;
       if (rel[i] > rel_tol) all = false;
-      // the normal residual goes to the low-precision pack through a staging
-      // buffer per rhs: stage in ehi (rn of this rhs), convert below
-      if ((rc = qb200_schur_apply(lat_hi, op_hi, -1, r, rn, tmp, st))) return rc;
-      double rnn;
-      if ((rc = qb200_blas_dot(QB200_F64, n1, rn, rn, scal, partials, st))) return rc;
-      if ((rc = fetch(&rnn, scal, 1, st))) return rc;
-      scale[i] = std::sqrt((double)n1 / (rnn > 0 ? rnn : 1.0));
-      // the scaled normal residual becomes slot i of the low-precision rhs
-      if ((rc = cuda_rc(mr_slot(true, lat_lo->ftype, n1, nrhs, i, rn, scale[i], rhs_lo, st), "multi-RHS pack slot")))
+      // slot i of r_lo: r scaled to unit rms per element
+      scale[i] = std::sqrt((double)n1 / (rr > 0 ? rr : 1.0));
+      if ((rc = cuda_rc(mr_slot(true, lat_lo->ftype, n1, nrhs, i, r, scale[i], r_lo, st), "multi-RHS pack slot")))
         return rc;
     }
     if (all || outer >= max_outer) break;
+    // normal-equation right-hand sides in the low precision: its rounding
+    // (~1e-3 relative for FP16) is far below the inner tolerance of a correction
+    if ((rc = mr_schur(lat_lo, nrhs, op_lo, 0, r_lo, rhs_lo, L.v[4], st))) return rc;
     if ((rc = cuda_rc(cudaMemsetAsync(e_lo, 0, lo_bytes, st), "mixed zero"))) return rc;
     int k = 0;
     double irel[kMaxRhs];
     if ((rc = mr_cg_core(lat_lo, nrhs, op_lo, rhs_lo, e_lo, inner_tol, max_inner, L, &k, irel, st))) return rc;
     tot += k;
-    for (int i = 0; i < nrhs; i++) {
-      if ((rc = cuda_rc(mr_slot(false, lat_lo->ftype, n1, nrhs, i, e_lo, 1.0 / scale[i], ehi, st),
-                        "multi-RHS unpack slot")))
+    for (int i = 0; i < nrhs; i++)
+      if ((rc = cuda_rc(mr_slot_add(lat_lo->ftype, n1, nrhs, i, e_lo, 1.0 / scale[i], x[i], st),
+                        "multi-RHS correction")))
         return rc;
-      if ((rc = qb200_blas_axpby(QB200_F64, n1, 1.0, ehi, 1.0, x[i], st))) return rc;
-    }
     outer++;
   }
   if (inner_iters) *inner_iters = tot;

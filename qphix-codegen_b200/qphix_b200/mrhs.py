@@ -75,8 +75,7 @@ def schur(op: EvenOddOperator, nrhs, x, isign=1, out=None, tmp=None):
 def cg(op: EvenOddOperator, nrhs, b, x=None, tol=1e-10, max_iter=10000):
     L = _lib.lib()
     x = x if x is not None else torch.zeros_like(b)
-    ws = torch.empty(L.qb200_cg_mrhs_workspace_bytes(ctypes.byref(op.lat), nrhs), dtype=torch.uint8,
-                     device=b.device)
+    ws = op.workspace("cg_mrhs", L.qb200_cg_mrhs_workspace_bytes(ctypes.byref(op.lat), nrhs))
     it = ctypes.c_int(0)
     rel = (ctypes.c_double * nrhs)()
     _lib.check(L.qb200_invert_cg_mrhs(ctypes.byref(op.lat), nrhs, ctypes.byref(op.op), b.data_ptr(), x.data_ptr(),
@@ -93,9 +92,8 @@ def mixed_solve(op_hi: EvenOddOperator, op_lo: EvenOddOperator, bs, tol=1e-10, i
     lo = ctypes.c_longlong(0)
     hi = L.qb200_mixed_mrhs_workspace_bytes(ctypes.byref(op_hi.lat), ctypes.byref(op_lo.lat), nrhs,
                                             ctypes.byref(lo))
-    dev = bs[0].device
-    ws_hi = torch.empty(hi, dtype=torch.uint8, device=dev)
-    ws_lo = torch.empty(lo.value, dtype=torch.uint8, device=dev)
+    ws_hi = op_hi.workspace("mixed_mrhs_hi", hi)
+    ws_lo = op_lo.workspace("mixed_mrhs_lo", lo.value)
     xs = [torch.zeros_like(b) for b in bs]
     ii, oo = ctypes.c_int(0), ctypes.c_int(0)
     rel = (ctypes.c_double * nrhs)()

@@ -7,7 +7,9 @@ libqphix_b200.so; see qb200_operator in include/qphix_b200.h).
 
 The target checkerboard is `target_cb` (1 = odd, as in QPhiX); `clov` and
 `gauge` are indexed by checkerboard.  Workspaces are allocated here with
-torch and passed down; the library itself allocates nothing.
+torch and passed down (the library itself allocates nothing); each operator
+keeps its solver workspaces between calls, so solves with one operator must
+run on one stream, one at a time.
 """
 import ctypes
 
@@ -50,12 +52,21 @@ class EvenOddOperator:
         self.op = op
         self.lat = g.c_struct()
         self.device = gauge[0].device
+        self._ws = {}
 
     def _spinor(self):
         return torch.zeros(self.g.spinor_elems, dtype=self.g.dtype, device=self.device)
 
     def _bytes(self, n):
         return torch.empty(int(n), dtype=torch.uint8, device=self.device)
+
+    def workspace(self, key, nbytes):
+        """Device byte buffer of at least nbytes, kept for later solves."""
+        t = self._ws.get(key)
+        if t is None or t.numel() < int(nbytes):
+            self._ws.pop(key, None)
+            t = self._ws[key] = self._bytes(nbytes)
+        return t
 
     def apply(self, x, isign=1, out=None, tmp=None):
         """out = Mhat x (isign +1) or Mhat^dag x (-1)."""
@@ -68,7 +79,7 @@ class EvenOddOperator:
     def _solve(self, fn, wsfn, b, x, tol, max_iter):
         L = _lib.lib()
         x = x if x is not None else self._spinor()
-        ws = self._bytes(getattr(L, wsfn)(ctypes.byref(self.lat)))
+        ws = self.workspace(wsfn, getattr(L, wsfn)(ctypes.byref(self.lat)))
         it = ctypes.c_int(0)
         rel = ctypes.c_double(0.0)
         _lib.check(getattr(L, fn)(ctypes.byref(self.lat), ctypes.byref(self.op), _ptr(b), _ptr(x), tol, max_iter,
@@ -96,7 +107,7 @@ def mixed_solve(op_hi: EvenOddOperator, op_lo: EvenOddOperator, b, solver="cg", 
     L = _lib.lib()
     lo = ctypes.c_longlong(0)
     hi = L.qb200_mixed_workspace_bytes(ctypes.byref(op_hi.lat), ctypes.byref(op_lo.lat), ctypes.byref(lo))
-    ws_hi, ws_lo = op_hi._bytes(hi), op_lo._bytes(lo.value)
+    ws_hi, ws_lo = op_hi.workspace("mixed_hi", hi), op_lo.workspace("mixed_lo", lo.value)
     x = x if x is not None else op_hi._spinor()
     ii, oo, rel = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_double(0.0)
     _lib.check(L.qb200_invert_mixed(ctypes.byref(op_hi.lat), ctypes.byref(op_hi.op), ctypes.byref(op_lo.lat),
