@@ -253,7 +253,7 @@ def bench_solve(dims, dev, nrhs=8, kappa=0.16):
     for nrhs Gaussian sources: (a) one FP64 CG per source, (b) FP32-corrected-
     by-FP64 CG per source, (c) all sources at once with FP16-storage multi-RHS
     corrections of FP64 solutions.  Each path runs once untimed first (module
-    loading, workspaces), then timed."""
+    loading, workspaces), then three times; the median is reported."""
     from qphix_b200 import fields, layout, mrhs
     from qphix_b200.lattice import F16, F32, F64, Geometry
     from qphix_b200.solver import EvenOddOperator, mixed_solve
@@ -281,21 +281,25 @@ def bench_solve(dims, dev, nrhs=8, kappa=0.16):
     mixed_solve(ops_[F64], ops_[F32], bs[0], tol=1e-4, inner_tol=1e-2)
     mrhs.mixed_solve(ops_[F64], ops_[F16], bs, tol=1e-3, inner_tol=1e-2)
 
-    def timed(fn):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        r = fn()
-        torch.cuda.synchronize()
-        return time.perf_counter() - t0, r
+    def timed(fn, reps=3):
+        """median wall time of reps runs (each synchronised) and the last result"""
+        ts = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return statistics.median(ts), r, ts
 
-    t64, r64 = timed(lambda: [ops_[F64].cg(b, tol=1e-10, max_iter=5000) for b in bs])
-    out["fp64_cg"] = {"seconds": t64, "iters": [r[1]["iters"] for r in r64],
+    t64, r64, a64 = timed(lambda: [ops_[F64].cg(b, tol=1e-10, max_iter=5000) for b in bs])
+    out["fp64_cg"] = {"seconds": t64, "runs": a64, "iters": [r[1]["iters"] for r in r64],
                       "max_rel_res": max(r[1]["rel_res"] for r in r64)}
-    t32, r32 = timed(lambda: [mixed_solve(ops_[F64], ops_[F32], b, tol=1e-10, inner_tol=1e-5) for b in bs])
-    out["fp32_fp64_single_rhs"] = {"seconds": t32, "inner_iters": [r[1]["inner_iters"] for r in r32],
+    t32, r32, a32 = timed(lambda: [mixed_solve(ops_[F64], ops_[F32], b, tol=1e-10, inner_tol=1e-5) for b in bs])
+    out["fp32_fp64_single_rhs"] = {"seconds": t32, "runs": a32, "inner_iters": [r[1]["inner_iters"] for r in r32],
                                    "max_rel_res": max(r[1]["rel_res"] for r in r32)}
-    t16, r16 = timed(lambda: mrhs.mixed_solve(ops_[F64], ops_[F16], bs, tol=1e-10, inner_tol=1e-2))
-    out["fp16_multi_rhs_mixed"] = {"seconds": t16, "inner_iters": r16[1]["inner_iters"],
+    t16, r16, a16 = timed(lambda: mrhs.mixed_solve(ops_[F64], ops_[F16], bs, tol=1e-10, inner_tol=1e-2))
+    out["fp16_multi_rhs_mixed"] = {"seconds": t16, "runs": a16, "inner_iters": r16[1]["inner_iters"],
                                    "outer_iters": r16[1]["outer_iters"], "max_rel_res": max(r16[1]["rel_res"])}
     out["speedup_vs_fp32_fp64_single_rhs"] = t32 / t16
     out["speedup_vs_fp64_cg"] = t64 / t16

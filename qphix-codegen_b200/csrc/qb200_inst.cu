@@ -58,8 +58,12 @@ cudaError_t go_pair(const KArgs<FT> &a, const GeoDev &g, const OpDev<float> &p, 
   const long long n = (long long)g.nxh * g.ny * (g.nrhs / 2);
   const dim3 grid((unsigned)((n + kThreads - 1) / kThreads), (unsigned)(g.nz * g.nt));
   if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
-  if (g.V == S) pair_dslash_kernel<FT, S, COMP12, FAM, ACH, S><<<grid, kThreads, 0, st>>>(a, g, p);
-  else pair_dslash_kernel<FT, S, COMP12, FAM, ACH, 0><<<grid, kThreads, 0, st>>>(a, g, p);
+  if (g.V != S) pair_dslash_kernel<FT, S, COMP12, FAM, ACH, 0, 0><<<grid, kThreads, 0, st>>>(a, g, p);
+  else if (g.nrhs == 2) pair_dslash_kernel<FT, S, COMP12, FAM, ACH, S, 2><<<grid, kThreads, 0, st>>>(a, g, p);
+  else if (g.nrhs == 4) pair_dslash_kernel<FT, S, COMP12, FAM, ACH, S, 4><<<grid, kThreads, 0, st>>>(a, g, p);
+  else if (g.nrhs == 8) pair_dslash_kernel<FT, S, COMP12, FAM, ACH, S, 8><<<grid, kThreads, 0, st>>>(a, g, p);
+  else if (g.nrhs == 16) pair_dslash_kernel<FT, S, COMP12, FAM, ACH, S, 16><<<grid, kThreads, 0, st>>>(a, g, p);
+  else pair_dslash_kernel<FT, S, COMP12, FAM, ACH, S, 0><<<grid, kThreads, 0, st>>>(a, g, p);
   return cudaGetLastError();
 }
 

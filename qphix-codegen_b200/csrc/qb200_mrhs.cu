@@ -492,7 +492,7 @@ int fetch(double *h, const double *d, int n, cudaStream_t st)
 // CG on Mhat^dag Mhat for nrhs systems at once (independent recurrences,
 // shared operator applications).  ws vectors: r, p, Ap, t, tmp.
 int mr_cg_core(const qb200_lattice *l, int nrhs, const qb200_operator *op, const void *rhs, void *x, double tol,
-               int max_iter, MRVecs &s, int *iters, double *rel, cudaStream_t st)
+               int max_iter, MRVecs &s, int *iters, double *rel, cudaStream_t st, bool x_zero = false)
 {
   MR m;
   m.ft = l->ftype;
@@ -502,10 +502,13 @@ int mr_cg_core(const qb200_lattice *l, int nrhs, const qb200_operator *op, const
   void *r = s.v[0], *p = s.v[1], *Ap = s.v[2], *t = s.v[3], *tmp = s.v[4];
   double *rr = s.slot(0), *rrn = s.slot(1), *pAp = s.slot(2), *bb = s.slot(3);
   int rc;
-  if ((rc = mr_schur(l, nrhs, op, 1, x, t, tmp, st))) return rc;
-  if ((rc = mr_schur(l, nrhs, op, 0, t, Ap, tmp, st))) return rc;
+  // r = rhs - A x (just rhs when the caller zeroed x)
+  if (!x_zero) {
+    if ((rc = mr_schur(l, nrhs, op, 1, x, t, tmp, st))) return rc;
+    if ((rc = mr_schur(l, nrhs, op, 0, t, Ap, tmp, st))) return rc;
+  }
   cudaError_t e = cudaMemcpyAsync(r, rhs, bytes, cudaMemcpyDeviceToDevice, st);
-  if (e == cudaSuccess) e = mr_axpby(m, vhost(-1.0), Ap, vhost(1.0), r, st);
+  if (e == cudaSuccess && !x_zero) e = mr_axpby(m, vhost(-1.0), Ap, vhost(1.0), r, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(p, r, bytes, cudaMemcpyDeviceToDevice, st);
   if (e == cudaSuccess) e = mr_dot(m, r, r, s.partials, rr, st);
   if (e == cudaSuccess) e = mr_dot(m, rhs, rhs, s.partials, bb, st);
@@ -688,7 +691,8 @@ int qb200_invert_mixed_mrhs(const qb200_lattice *lat_hi, const qb200_operator *o
     if ((rc = cuda_rc(cudaMemsetAsync(e_lo, 0, lo_bytes, st), "mixed zero"))) return rc;
     int k = 0;
     double irel[kMaxRhs];
-    if ((rc = mr_cg_core(lat_lo, nrhs, op_lo, rhs_lo, e_lo, inner_tol, max_inner, L, &k, irel, st))) return rc;
+    if ((rc = mr_cg_core(lat_lo, nrhs, op_lo, rhs_lo, e_lo, inner_tol, max_inner, L, &k, irel, st, true)))
+      return rc;
     tot += k;
     for (int i = 0; i < nrhs; i++)
       if ((rc = cuda_rc(mr_slot_add(lat_lo->ftype, n1, nrhs, i, e_lo, 1.0 / scale[i], x[i], st),

@@ -20,10 +20,15 @@
 
 #include "qb200_site_kernel.cuh"
 
-// minimum resident blocks of 128 threads per SM the register allocation
-// must allow
-#ifndef QB_PAIR_MINB
-#define QB_PAIR_MINB 1
+// minimum resident blocks of 128 threads per SM the register allocation must
+// allow: the achimbdpsi form (chi and the clover block live next to the
+// accumulators) gains from a cap at 128 registers, the plain form and the
+// dense twisted-mass-clover block (which would spill under the cap) do not
+#ifndef QB_PAIR_MINB_ACH
+#define QB_PAIR_MINB_ACH 4
+#endif
+#ifndef QB_PAIR_MINB_PLAIN
+#define QB_PAIR_MINB_PLAIN 1
 #endif
 
 namespace qb200 {
@@ -265,12 +270,15 @@ __device__ __forceinline__ void hops2(const KArgs<FT> &a, const GeoDev &g, const
 }
 
 // Grid: blockIdx.y = the (z, t) plane; x covers the plane's sites times
-// nrhs/2 pairs (pair fastest).  Requires an even nrhs.
-template <typename FT, int S, bool COMP12, int FAM, bool ACH, int VV>
-__global__ void __launch_bounds__(128, QB_PAIR_MINB)
+// nrhs/2 pairs (pair fastest).  Requires an even nrhs.  NR: nrhs fixed at
+// compile time (so every spinor component sits at a constant offset from the
+// site's base), or 0 for the run-time g.nrhs.
+template <typename FT, int S, bool COMP12, int FAM, bool ACH, int VV, int NR>
+__global__ void __launch_bounds__(128, (ACH && FAM != FAM_TMCLOV) ? QB_PAIR_MINB_ACH : QB_PAIR_MINB_PLAIN)
     pair_dslash_kernel(const KArgs<FT> a, const GeoDev g, const OpDev<float> p)
 {
-  const int np = g.nrhs >> 1;
+  const int nr = NR ? NR : g.nrhs;
+  const int np = nr >> 1;
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= g.nxh * g.ny * np) return;
   const int sp = q / np;
@@ -286,10 +294,13 @@ __global__ void __launch_bounds__(128, QB_PAIR_MINB)
   constexpr int R = COMP12 ? 2 : 3;
   const int V = vlen<VV>(g);
   const long long gbase = tile * (8LL * R * 6 * V) + lane;
-  const long long obase = spinor_base_mr<S>(g, s, 2 * rp);
-  const long long ue = 24LL * S * g.nrhs;
-  const int le = g.nrhs;
-  const int cs = S * g.nrhs;
+  // multi-RHS block FT[3][4][2][S][nrhs]: component k of lane l, rhs r at
+  // blk*24*S*nrhs + k*S*nrhs + l*nrhs + r
+  const long long blk = s.t * g.Pxyz + s.z * g.Pxy + (long long)s.y * g.nvecs + s.xcb / S;
+  const long long obase = (blk * (24 * S) + (s.xcb % S)) * nr + 2 * rp;
+  const long long ue = 24LL * S * nr;
+  const int le = nr;
+  const int cs = S * nr;
 
   c2 res[4][3];
   if (ACH) {

@@ -426,15 +426,16 @@ int normal_op(const qb200_lattice *l, const qb200_operator *op, const void *v, v
 // (alpha = rr/pAp and beta = rr_new/rr are formed inside the axpby
 // kernels); the host reads |r|^2 once per iteration for the stopping test.
 int cg_core(const qb200_lattice *l, const qb200_operator *op, const void *rhs, void *x, double tol, int max_iter,
-            const Vecs &s, int *iters, double *rel, cudaStream_t st)
+            const Vecs &s, int *iters, double *rel, cudaStream_t st, bool x_zero = false)
 {
   const VS V = vs_of(l);
   void *r = s.v[0], *p = s.v[1], *Ap = s.v[2], *t = s.v[3], *tmp = s.v[4];
   double *rr_d = s.scal + 0, *rrn_d = s.scal + 1, *pAp_d = s.scal + 2, *bb_d = s.scal + 3;
   int rc;
-  if ((rc = normal_op(l, op, x, Ap, t, tmp, st))) return rc;
+  // r = rhs - A x (just rhs when the caller zeroed x)
+  if (!x_zero && (rc = normal_op(l, op, x, Ap, t, tmp, st))) return rc;
   if ((rc = copy(r, rhs, spinor_bytes(l), st))) return rc;
-  cudaError_t e = axpby(V, host(-1.0), Ap, host(1.0), r, st);
+  cudaError_t e = x_zero ? cudaSuccess : axpby(V, host(-1.0), Ap, host(1.0), r, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(p, r, spinor_bytes(l), cudaMemcpyDeviceToDevice, st);
   if (e == cudaSuccess) e = dot(V, r, r, s.partials, rr_d, st);
   if (e == cudaSuccess) e = dot(V, rhs, rhs, s.partials, bb_d, st);
@@ -828,7 +829,7 @@ int qb200_invert_mixed(const qb200_lattice *lat_hi, const qb200_operator *op_hi,
     if ((rc = cuda_rc(e, "mixed demote"))) return rc;
     int k = 0;
     double irel = 0.0;
-    if (solver == 0) rc = cg_core(lat_lo, op_lo, rhs_lo, e_lo, inner_tol, max_inner, L, &k, &irel, st);
+    if (solver == 0) rc = cg_core(lat_lo, op_lo, rhs_lo, e_lo, inner_tol, max_inner, L, &k, &irel, st, true);
     else rc = bicgstab_core(lat_lo, op_lo, rhs_lo, e_lo, inner_tol, max_inner, L, &k, &irel, st);
     if (rc) return rc;
     tot += k;
