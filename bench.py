@@ -346,6 +346,48 @@ def bench_force(dev, dims=(24, 24, 24, 48)):
             "note": "autograd step = forward dslash + dagger dslash + force + torch packing/folding of links"}
 
 
+def bench_batch(dev, peak):
+    """Clover A.chi - b.D.psi (FP32, 12-real links, SOALEN = VECLEN = 4) over
+    the uneven batch 3 x 16^3x32 + 2 x 24^3x48 + 1 x 32^3x64 (seeded random
+    fields; 960 algorithmic bytes and 1824 flop per site): one launch per
+    lattice, one batched launch (one thread per site), the tuned batched
+    launch, and ten tuned launches replayed from a CUDA graph."""
+    from qphix_b200 import batch, ops
+    from qphix_b200.lattice import F32, Geometry
+    dims = [(16, 16, 16, 32)] * 3 + [(24, 24, 24, 48)] * 2 + [(32, 32, 32, 64)]
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(95)
+    probs = []
+    for d in dims:
+        g = Geometry(*d, soalen=4, veclen=4, ftype=F32, compress12=True, t_boundary=-1.0)
+        r = lambda n: torch.randn(n, generator=gen, device=dev)  # noqa: E731
+        probs.append(batch.Problem(g, 0, r(g.spinor_elems), torch.zeros(g.spinor_elems, device=dev),
+                                   r(g.gauge_elems), chi=r(g.spinor_elems), clover=r(g.clover_elems), **PARAMS))
+    sites = sum(p.g.vol_cb for p in probs)
+    stream = torch.cuda.current_stream()
+    op = batch.BatchedDslash("clover", "achimbdpsi", 1, probs)
+
+    def seq():
+        for p in probs:
+            ops.dslash(p.g, "clover", "achimbdpsi", 1, 0, p.psi, p.out, p.gauge, chi=p.chi, clover=p.clover,
+                       **PARAMS)
+
+    res = {"lattices": ["x".join(map(str, d)) for d in dims], "sites": sites, "bytes_per_site": 960}
+    t_seq = _time(seq, 20, stream)
+    t_one = _time(lambda: op(grid=0, block=128), 20, stream)
+    grid, block, _ = op.tune()
+    t_tuned = _time(op, 20, stream)
+    graph = op.capture(steps=10)
+    t_graph = _time(graph.replay, 5, stream) / 10
+    for name, t in (("per_lattice_launches", t_seq), ("batched_one_thread_per_site", t_one),
+                    ("batched_tuned", t_tuned), ("batched_tuned_graph", t_graph)):
+        gbs = 960 * sites / (t * 1e-3) / 1e9
+        res[name] = {"ms": t, "gflops": FLOP_SITE * sites / (t * 1e-3) / 1e9, "gbs": gbs, "frac_of_peak": gbs / peak}
+    res["tuned_launch"] = {"grid": grid, "block": block}
+    del graph
+    return res
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -498,6 +540,7 @@ def b200_arm(args, world, rank, local):
         extras["mrhs"] = bench_mrhs(g, f, dev)
         extras["solve"] = bench_solve(dims, dev)
         extras["force"] = bench_force(dev)
+        extras["batch"] = bench_batch(dev, peak)
 
     if rank == 0:
         line = {

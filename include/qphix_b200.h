@@ -462,6 +462,45 @@ int qb200_invert_mixed_mrhs(const qb200_lattice *lat_hi, const qb200_operator *o
                             double rel_tol, double inner_tol, int max_inner, int max_outer, void *ws_hi, void *ws_lo,
                             int *inner_iters, int *outer_iters, double *rel_res, void *stream);
 
+/* ---- batched launch and launch tuning -----------------------------------
+ * No counterpart in the reference (its kernels cover one tile of one lattice
+ * per call).  One launch applies the same operator (family 0..3 as in
+ * qb200_operator, achimbdpsi 0/1, isign) to up to QB200_MAX_BATCH independent
+ * lattices of possibly different sizes.  All items share ftype, soalen,
+ * veclen and compress12 (soalen >= 4 needs veclen == soalen); each has its
+ * own fields, checkerboard and coefficients (qb200_coeffs; hops leaving a
+ * lattice wrap around it: every accumulate flag is on).  The per-site
+ * operator is that of the single-lattice entry points. */
+#define QB200_MAX_BATCH 16
+typedef struct qb200_batch_item {
+  qb200_lattice lat;
+  int cb;
+  const void *psi, *chi, *gauge, *clov; /* chi: achimbdpsi only; clov: clover families */
+  void *out;
+  qb200_coeffs coeffs;
+} qb200_batch_item;
+/* grid = number of blocks (0: one thread per site; smaller grids make the
+ * threads stride through the sites: a persistent launch); block = 64 or 128 */
+typedef struct qb200_launch_cfg {
+  int grid, block;
+} qb200_launch_cfg;
+/* cfg NULL: the tuned choice for this batch if qb200_tune_batched has seen
+ * its key (operator, layout, lattice sizes, device), else one thread per
+ * site with blocks of 128 */
+int qb200_dslash_batched(int family, int achimbdpsi, int isign, int nitems, const qb200_batch_item *items,
+                         const qb200_launch_cfg *cfg, void *stream);
+/* times the candidate launch configurations on these fields (each run
+ * writes the operator's result to the items' out), remembers the fastest
+ * under the batch's key and returns it; a key already tuned returns at once.
+ * Synchronises the stream; do not call it during stream capture. */
+int qb200_tune_batched(int family, int achimbdpsi, int isign, int nitems, const qb200_batch_item *items,
+                       qb200_launch_cfg *best, double *best_ms, void *stream);
+/* the process-wide tuning table as text lines "key grid block ms";
+ * load returns the number of entries read or a negative status */
+int qb200_tune_cache_save(const char *path);
+int qb200_tune_cache_load(const char *path);
+void qb200_tune_cache_clear(void);
+
 /* ---- backward: link derivative of the hopping term ----------------------
  * No counterpart in the reference (it has no backward kernels).
  *

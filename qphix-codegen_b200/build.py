@@ -41,7 +41,8 @@ def units():
     out = [(os.path.join(BUILD, "qb200_api.o"), [], os.path.join(CSRC, "qb200_api.cu")),
            (os.path.join(BUILD, "qb200_solver.o"), [], os.path.join(CSRC, "qb200_solver.cu")),
            (os.path.join(BUILD, "qb200_mrhs.o"), [], os.path.join(CSRC, "qb200_mrhs.cu")),
-           (os.path.join(BUILD, "qb200_force.o"), [], os.path.join(CSRC, "qb200_force.cu"))]
+           (os.path.join(BUILD, "qb200_force.o"), [], os.path.join(CSRC, "qb200_force.cu")),
+           (os.path.join(BUILD, "qb200_batch.o"), [], os.path.join(CSRC, "qb200_batch.cu"))]
     for tag, ft in FTYPES.items():
         for s in SOALENS:
             if tag in WIDE_ONLY and s < 4:

@@ -323,6 +323,12 @@ void api_fill_op_f(OpDev<float> &p, const qb200_lattice *l, int isPlus, int cb, 
   fill_op<float>(p, l, isPlus, cb, negate, cs, ctf, ctb, tbc_mask, ph, acc);
 }
 
+void api_fill_op_d(OpDev<double> &p, const qb200_lattice *l, int isPlus, int cb, bool negate, double cs, double ctf,
+                   double ctb, unsigned tbc_mask, const double *ph, const unsigned *acc)
+{
+  fill_op<double>(p, l, isPlus, cb, negate, cs, ctf, ctb, tbc_mask, ph, acc);
+}
+
 int api_body(const qb200_lattice *l, int fam, bool ach, int isPlus, int cb, const void *psi, const void *chi,
              const void *gauge, const void *clov, void *out, const unsigned *accumulate, double coeff_s,
              double coeff_t_f, double coeff_t_b, unsigned tbc_mask, const double *tbc_phases, double alpha,

@@ -94,6 +94,15 @@ cudaError_t go_unpack(const elem_t<FT> *buf, const elem_t<FT> *gauge, const elem
   return cudaGetLastError();
 }
 
+template <typename FT, int S, bool COMP12, int FAM, bool ACH>
+cudaError_t go_batch(const BatchDev<FT> &b, bool vfixed, int grid, int block, cudaStream_t st)
+{
+  if (S >= 4 && vfixed) batch_dslash_kernel<FT, S, COMP12, FAM, ACH, (S >= 4 ? S : 0)><<<grid, block, 0, st>>>(b);
+  else if (S < 4) batch_dslash_kernel<FT, S, COMP12, FAM, ACH, 0><<<grid, block, 0, st>>>(b);
+  else return cudaErrorInvalidValue; // SOALEN >= 4 layouts batch only with VECLEN == SOALEN
+  return cudaGetLastError();
+}
+
 FaceDev to_dev(const FaceSpec &s)
 {
   FaceDev f;
@@ -142,6 +151,32 @@ cudaError_t launch_dslash_mrhs(const LaunchSpec &ls, const elem_t<FT> *psi, cons
 #endif
 
 template <typename FT, int S>
+cudaError_t launch_dslash_batched(const LaunchSpec &ls, const BatchDev<FT> &b, bool vfixed, int grid, int block,
+                                  cudaStream_t st)
+{
+  if (b.total == 0) return cudaSuccess;
+  switch (ls.fam * 4 + (ls.ach ? 2 : 0) + (ls.comp12 ? 1 : 0)) {
+  case 0: return go_batch<FT, S, false, FAM_WILSON, false>(b, vfixed, grid, block, st);
+  case 1: return go_batch<FT, S, true, FAM_WILSON, false>(b, vfixed, grid, block, st);
+  case 2: return go_batch<FT, S, false, FAM_WILSON, true>(b, vfixed, grid, block, st);
+  case 3: return go_batch<FT, S, true, FAM_WILSON, true>(b, vfixed, grid, block, st);
+  case 4: return go_batch<FT, S, false, FAM_CLOVER, false>(b, vfixed, grid, block, st);
+  case 5: return go_batch<FT, S, true, FAM_CLOVER, false>(b, vfixed, grid, block, st);
+  case 6: return go_batch<FT, S, false, FAM_CLOVER, true>(b, vfixed, grid, block, st);
+  case 7: return go_batch<FT, S, true, FAM_CLOVER, true>(b, vfixed, grid, block, st);
+  case 8: return go_batch<FT, S, false, FAM_TM, false>(b, vfixed, grid, block, st);
+  case 9: return go_batch<FT, S, true, FAM_TM, false>(b, vfixed, grid, block, st);
+  case 10: return go_batch<FT, S, false, FAM_TM, true>(b, vfixed, grid, block, st);
+  case 11: return go_batch<FT, S, true, FAM_TM, true>(b, vfixed, grid, block, st);
+  case 12: return go_batch<FT, S, false, FAM_TMCLOV, false>(b, vfixed, grid, block, st);
+  case 13: return go_batch<FT, S, true, FAM_TMCLOV, false>(b, vfixed, grid, block, st);
+  case 14: return go_batch<FT, S, false, FAM_TMCLOV, true>(b, vfixed, grid, block, st);
+  case 15: return go_batch<FT, S, true, FAM_TMCLOV, true>(b, vfixed, grid, block, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <typename FT, int S>
 cudaError_t launch_face_pack(const elem_t<FT> *psi, elem_t<FT> *buf, const GeoDev &g, const FaceSpec &fs,
                              int isPlus, cudaStream_t st)
 {
@@ -176,6 +211,8 @@ typedef elem_t<QB_FT> QB_E;
 template cudaError_t launch_dslash<QB_FT, QB_S>(const LaunchSpec &, const QB_E *, const QB_E *, const QB_E *,
                                                 const QB_E *, QB_E *, const GeoDev &, const OpDev<comp_t<QB_FT>> &,
                                                 cudaStream_t);
+template cudaError_t launch_dslash_batched<QB_FT, QB_S>(const LaunchSpec &, const BatchDev<QB_FT> &, bool, int, int,
+                                                        cudaStream_t);
 template cudaError_t launch_face_pack<QB_FT, QB_S>(const QB_E *, QB_E *, const GeoDev &, const FaceSpec &, int,
                                                    cudaStream_t);
 #if QB_MRHS

@@ -5,7 +5,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
-#include "qb200_device.cuh"
+#include "qb200_site_kernel.cuh"
 
 namespace qb200 {
 
@@ -28,6 +28,13 @@ template <typename FT, int S>
 cudaError_t launch_dslash_mrhs(const LaunchSpec &ls, const elem_t<FT> *psi, const elem_t<FT> *chi,
                                const elem_t<FT> *gauge, const elem_t<FT> *clov, elem_t<FT> *out, const GeoDev &g,
                                const OpDev<comp_t<FT>> &p, cudaStream_t st);
+
+// batched launcher (qb200_site_kernel.cuh: batch_dslash_kernel), defined in
+// qb200_inst.cu for each (FT, S); vfixed: every item has VECLEN == SOALEN
+// (compile-time VECLEN for S >= 4); block <= 128
+template <typename FT, int S>
+cudaError_t launch_dslash_batched(const LaunchSpec &ls, const BatchDev<FT> &b, bool vfixed, int grid, int block,
+                                  cudaStream_t st);
 
 // face launchers, defined in qb200_inst.cu for each (FT, S)
 struct FaceSpec {

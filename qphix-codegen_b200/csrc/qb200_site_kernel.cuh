@@ -98,26 +98,14 @@ __device__ __forceinline__ void do_hop(const KArgs<FT> &a, const GeoDev &g,
   recons<C, MU>(ub, beta, tau, acc);
 }
 
-// Grid: blockIdx.y = the (z, t) plane, x covers the plane's sites (times the
-// right-hand sides).  MR: multi-RHS layout, one thread per (site, right-hand
-// side) with the right-hand side fastest, so the nrhs threads of a site share
-// each link and clover load.
+// The operator at one output site s (and right-hand side rhs of the
+// multi-RHS layout when MR).
 template <typename FT, int S, bool COMP12, int FAM, bool ACH, bool MR, int VV>
-__global__ void __launch_bounds__(128)
-    site_dslash_kernel(const KArgs<FT> a, const GeoDev g, const OpDev<typename ftraits<FT>::C> p)
+__device__ __forceinline__ void site_body(const KArgs<FT> &a, const GeoDev &g,
+                                          const OpDev<typename ftraits<FT>::C> &p, const Site &s, int rhs)
 {
   typedef typename ftraits<FT>::C C;
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
   const int nr = MR ? g.nrhs : 1;
-  if (q >= g.nxh * g.ny * nr) return;
-  const int sp = MR ? q / nr : q;
-  const int rhs = MR ? q - sp * nr : 0;
-  Site s;
-  s.z = blockIdx.y % g.nz;
-  s.t = blockIdx.y / g.nz;
-  s.y = sp / g.nxh;
-  s.xcb = sp - s.y * g.nxh;
-  s.par = (s.y + s.z + s.t + p.cb) & 1;
   int lane;
   const long long tile = tile_of<S>(g, s, &lane);
   constexpr int R = COMP12 ? 2 : 3;
@@ -213,6 +201,60 @@ __global__ void __launch_bounds__(128)
   }
   if (MR) store_spinor_rs<FT>(a.out, obase, cs, res);
   else store_spinor<FT, S>(a.out, obase, res);
+}
+
+// Grid: blockIdx.y = the (z, t) plane, x covers the plane's sites (times the
+// right-hand sides).  MR: multi-RHS layout, one thread per (site, right-hand
+// side) with the right-hand side fastest, so the nrhs threads of a site share
+// each link and clover load.
+template <typename FT, int S, bool COMP12, int FAM, bool ACH, bool MR, int VV>
+__global__ void __launch_bounds__(128)
+    site_dslash_kernel(const KArgs<FT> a, const GeoDev g, const OpDev<typename ftraits<FT>::C> p)
+{
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nr = MR ? g.nrhs : 1;
+  if (q >= g.nxh * g.ny * nr) return;
+  const int sp = MR ? q / nr : q;
+  const int rhs = MR ? q - sp * nr : 0;
+  Site s;
+  s.z = blockIdx.y % g.nz;
+  s.t = blockIdx.y / g.nz;
+  s.y = sp / g.nxh;
+  s.xcb = sp - s.y * g.nxh;
+  s.par = (s.y + s.z + s.t + p.cb) & 1;
+  site_body<FT, S, COMP12, FAM, ACH, MR, VV>(a, g, p, s, rhs);
+}
+
+// Several lattices (a batch of independent problems with the same storage
+// type and layout) in one launch.  Work unit u of the flattened index space
+// is site u - first[k] of item k; with a grid smaller than the work the
+// threads stride through it (persistent launch).
+constexpr int kMaxBatch = 16;
+
+template <typename FT> struct BatchItem {
+  KArgs<FT> a;
+  GeoDev g;
+  OpDev<typename ftraits<FT>::C> p;
+  long long first; // first work unit of the item
+};
+
+template <typename FT> struct BatchDev {
+  BatchItem<FT> it[kMaxBatch];
+  int n;
+  long long total;
+};
+
+template <typename FT, int S, bool COMP12, int FAM, bool ACH, int VV>
+__global__ void __launch_bounds__(128) batch_dslash_kernel(const __grid_constant__ BatchDev<FT> b)
+{
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < b.total; u += stride) {
+    int k = 0;
+    while (k + 1 < b.n && u >= b.it[k + 1].first) k++;
+    const BatchItem<FT> &it = b.it[k];
+    const Site s = site_of(it.g, (int)(u - it.first), it.p.cb);
+    site_body<FT, S, COMP12, FAM, ACH, false, VV>(it.a, it.g, it.p, s, 0);
+  }
 }
 
 } // namespace qb200

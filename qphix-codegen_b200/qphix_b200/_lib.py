@@ -126,6 +126,33 @@ INFO.update({
 SIGNATURES.update({
     "qb200_hop_force": [_LAT, _I, _I, _P, _P, _P, _D, _D, _D, _U, _DA, _P, _P],
 })
+
+
+class BatchItem(ctypes.Structure):
+    """ctypes mirror of `qb200_batch_item`."""
+    _fields_ = [
+        ("lat", Lattice), ("cb", ctypes.c_int),
+        ("psi", ctypes.c_void_p), ("chi", ctypes.c_void_p), ("gauge", ctypes.c_void_p), ("clov", ctypes.c_void_p),
+        ("out", ctypes.c_void_p), ("coeffs", Coeffs),
+    ]
+
+
+class LaunchCfg(ctypes.Structure):
+    """ctypes mirror of `qb200_launch_cfg`."""
+    _fields_ = [("grid", ctypes.c_int), ("block", ctypes.c_int)]
+
+
+MAX_BATCH = 16
+_BIP = ctypes.POINTER(BatchItem)
+SIGNATURES.update({
+    "qb200_dslash_batched": [_I, _I, _I, _I, _BIP, ctypes.POINTER(LaunchCfg), _P],
+    "qb200_tune_batched": [_I, _I, _I, _I, _BIP, ctypes.POINTER(LaunchCfg), _DP, _P],
+    "qb200_tune_cache_save": [ctypes.c_char_p],
+    "qb200_tune_cache_load": [ctypes.c_char_p],
+})
+INFO.update({
+    "qb200_tune_cache_clear": ([], None),
+})
 INFO.update({
     "qb200_hop_force_elems": ([_LAT], _LL),
 })
