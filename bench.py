@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bound of the CPU baseline sample")
     ap.add_argument("--no-extras", action="store_true", help="skip the multi-RHS and solver measurements")
+    ap.add_argument("--only", choices=["mrhs", "force", "batch", "solve"],
+                    help="run one secondary measurement alone (on --dims) and print its JSON line")
     return ap.parse_args()
 
 
@@ -492,6 +494,8 @@ def b200_arm(args, world, rank, local):
     if world == 1 and args.e2e_steps > 0:
         hpsi = f["psi"].cpu().pin_memory()
         hchi = f["chi"].cpu().pin_memory()
+        nb = f["psi"].numel() * 4
+        # serial: each step copies in, computes and copies out on one stream
         hout = torch.empty_like(hpsi).pin_memory()
         dpsi, dchi = torch.empty_like(f["psi"]), torch.empty_like(f["chi"])
 
@@ -511,11 +515,52 @@ def b200_arm(args, world, rank, local):
             e2e_step()
         a1.record(stream)
         torch.cuda.synchronize()
-        e_ms = a0.elapsed_time(a1) / args.e2e_steps
-        nb = f["psi"].numel() * 4
+        serial_ms = a0.elapsed_time(a1) / args.e2e_steps
+        # pipelined: double buffers on three streams, so that the host-to-device
+        # copies of step i+1 overlap the device-to-host copy of step i (the PCIe
+        # link carries both directions at once)
+        s_in, s_run, s_out = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+        bufs = [(torch.empty_like(f["psi"]), torch.empty_like(f["chi"]), torch.empty_like(out),
+                 torch.empty_like(hpsi).pin_memory()) for _ in range(2)]
+        ev_in = [torch.cuda.Event() for _ in range(2)]
+        ev_run = [torch.cuda.Event() for _ in range(2)]
+        ev_out = [torch.cuda.Event() for _ in range(2)]
+
+        def pipelined(nsteps):
+            for i in range(nsteps):
+                b = i % 2
+                bp, bc, bo, bh = bufs[b]
+                if i >= 2:
+                    s_in.wait_event(ev_run[b])          # step i-2 has read this input buffer
+                with torch.cuda.stream(s_in):
+                    bp.copy_(hpsi, non_blocking=True)
+                    bc.copy_(hchi, non_blocking=True)
+                    ev_in[b].record(s_in)
+                s_run.wait_event(ev_in[b])
+                if i >= 2:
+                    s_run.wait_event(ev_out[b])         # step i-2's result has left this buffer
+                ops.dslash(g, "clover", "achimbdpsi", 1, 0, bp, bo, f["gauge"], chi=bc, clover=f["clover"],
+                           stream=s_run, **PARAMS)
+                ev_run[b].record(s_run)
+                s_out.wait_event(ev_run[b])
+                with torch.cuda.stream(s_out):
+                    bh.copy_(bo, non_blocking=True)
+                    ev_out[b].record(s_out)
+
+        pipelined(2)
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(s_in)
+        pipelined(args.e2e_steps)
+        p1.record(s_out)
+        torch.cuda.synchronize()
+        e_ms = p0.elapsed_time(p1) / args.e2e_steps
+        assert torch.equal(bufs[(args.e2e_steps - 1) % 2][3], hout), "pipelined result differs from the serial one"
         e2e = {"value": FLOP_SITE * g.vol_cb / (e_ms * 1e-3) / 1e9, "unit": "GFLOP/s",
                "h2d_bytes_per_step": 2 * nb, "d2h_bytes_per_step": nb, "ms_per_step": e_ms,
-               "path": "qb200_clov_dslash_achimbdpsi_plus_vec via ctypes, pinned host buffers"}
+               "serial_ms_per_step": serial_ms,
+               "path": ("qb200_clov_dslash_achimbdpsi_plus_vec via ctypes, pinned host buffers; psi and chi "
+                        "copied in and out copied back every step, double-buffered over steps")}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -567,8 +612,28 @@ def b200_arm(args, world, rank, local):
         dist.barrier()
 
 
+def run_only(args):
+    """One secondary measurement alone, for profiling it on a chosen size."""
+    dev = torch.device("cuda", 0)
+    dims = tuple(int(x) for x in args.dims.split(","))
+    if args.only == "mrhs":
+        from qphix_b200.lattice import F32, Geometry
+        g = Geometry(*dims, soalen=args.soalen, veclen=args.veclen, ftype=F32, compress12=True, t_boundary=-1.0)
+        r = bench_mrhs(g, make_fields(g, dev), dev)
+    elif args.only == "force":
+        r = bench_force(dev, dims)
+    elif args.only == "batch":
+        r = bench_batch(dev, measured_peak()[0])
+    else:
+        r = bench_solve(dims, dev)
+    print(json.dumps({"only": args.only, "dims": list(dims), "result": r}))
+
+
 def main():
     args = parse()
+    if args.only:
+        run_only(args)
+        return
     world, rank, local = dist_setup(args)
     try:
         if args.impl == "reference":
