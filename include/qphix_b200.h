@@ -462,6 +462,28 @@ int qb200_invert_mixed_mrhs(const qb200_lattice *lat_hi, const qb200_operator *o
                             double rel_tol, double inner_tol, int max_inner, int max_outer, void *ws_hi, void *ws_lo,
                             int *inner_iters, int *outer_iters, double *rel_res, void *stream);
 
+/* ---- layout converters -------------------------------------------------
+ * No counterpart in the reference (QPhiX converts on the host).  Canonical
+ * site-major complex fields in device memory, (re, im) pairs of ctype =
+ * QB200_F64 or QB200_F32:
+ *   spinor  [nt][nz][ny][nxh][4 spin][3 colour]            one checkerboard
+ *   links   [4 mu][nt_global][nz][ny][nx][3][3] (U)         the whole lattice
+ *   clover  [nt][nz][ny][nxh][2 block][6][6]                one checkerboard
+ * (site (xcb, y, z, t) of checkerboard cb at x = 2*xcb + ((y+z+t+cb)&1)),
+ * to and from the tile layouts of lat (storage type lat->ftype; QB200_F16N
+ * spinors get their per-site norm).  Padding blocks of a spinor field are
+ * not written: zero the field once.  qb200_pack_gauge packs the links of
+ * checkerboard cb of the local slab whose first time slice is global slice
+ * t0 (G = U^T, backward links U(x - mu), rows 0-1 when compress12);
+ * qb200_pack_clover keeps the diagonal and lower triangle of each Hermitian
+ * block, qb200_pack_full_clover the dense blocks. */
+int qb200_pack_spinor(const qb200_lattice *lat, int ctype, const void *canon, void *spinor, void *stream);
+int qb200_unpack_spinor(const qb200_lattice *lat, int ctype, const void *spinor, void *canon, void *stream);
+int qb200_pack_gauge(const qb200_lattice *lat, int cb, int ctype, const void *links, int nt_global, int t0,
+                     void *gauge, void *stream);
+int qb200_pack_clover(const qb200_lattice *lat, int ctype, const void *blocks, void *clover, void *stream);
+int qb200_pack_full_clover(const qb200_lattice *lat, int ctype, const void *blocks, void *clover, void *stream);
+
 /* ---- batched launch and launch tuning -----------------------------------
  * No counterpart in the reference (its kernels cover one tile of one lattice
  * per call).  One launch applies the same operator (family 0..3 as in

@@ -42,7 +42,8 @@ def units():
            (os.path.join(BUILD, "qb200_solver.o"), [], os.path.join(CSRC, "qb200_solver.cu")),
            (os.path.join(BUILD, "qb200_mrhs.o"), [], os.path.join(CSRC, "qb200_mrhs.cu")),
            (os.path.join(BUILD, "qb200_force.o"), [], os.path.join(CSRC, "qb200_force.cu")),
-           (os.path.join(BUILD, "qb200_batch.o"), [], os.path.join(CSRC, "qb200_batch.cu"))]
+           (os.path.join(BUILD, "qb200_batch.o"), [], os.path.join(CSRC, "qb200_batch.cu")),
+           (os.path.join(BUILD, "qb200_convert.o"), [], os.path.join(CSRC, "qb200_convert.cu"))]
     for tag, ft in FTYPES.items():
         for s in SOALENS:
             if tag in WIDE_ONLY and s < 4:
@@ -77,7 +78,8 @@ def compile_one(obj, extra, src, log):
 def build(jobs=None, force=False, verbose=True):
     os.makedirs(BUILD, exist_ok=True)
     src_t = newest_source()
-    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= src_t:
+    if (not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= src_t
+            and all(os.path.exists(u[0]) and os.path.getmtime(u[0]) <= os.path.getmtime(LIB) for u in units())):
         return LIB
     jobs = jobs or max(1, os.cpu_count() or 1)
     todo = []

@@ -28,7 +28,9 @@ enum { FAM_WILSON = 0, FAM_CLOVER = 1, FAM_TM = 2, FAM_TMCLOV = 3 };
 // storage traits.  FT names the storage format, E the element type in
 // memory, C the arithmetic type; SPB is the number of E elements per site
 // lane of a spinor block (24, or 26 when two extra halves hold the site's
-// FP32 norm) and FACE the elements per face site.
+// FP32 norm) and FACE the elements per face site.  ld reads global memory
+// through the read-only path, cv converts an element already loaded (from
+// shared memory, say).
 
 // FP16 spinors scaled by a per-site FP32 norm (links and clover plain FP16):
 // block = FT[3][4][2][S] halves followed by float norm[S].  WIDE_ONLY types
@@ -42,6 +44,7 @@ template <> struct ftraits<float> {
   static constexpr int SPB = 24, FACE = 12;
   static constexpr bool WIDE_ONLY = false;
   static __device__ __forceinline__ float ld(const float *p) { return __ldg(p); }
+  static __device__ __forceinline__ float cv(float v) { return v; }
   static __device__ __forceinline__ void st(float *p, float v) { *p = v; }
 };
 template <> struct ftraits<double> {
@@ -50,6 +53,7 @@ template <> struct ftraits<double> {
   static constexpr int SPB = 24, FACE = 12;
   static constexpr bool WIDE_ONLY = false;
   static __device__ __forceinline__ double ld(const double *p) { return __ldg(p); }
+  static __device__ __forceinline__ double cv(double v) { return v; }
   static __device__ __forceinline__ void st(double *p, double v) { *p = v; }
 };
 template <> struct ftraits<__half> {
@@ -58,6 +62,7 @@ template <> struct ftraits<__half> {
   static constexpr int SPB = 24, FACE = 12;
   static constexpr bool WIDE_ONLY = false;
   static __device__ __forceinline__ float ld(const __half *p) { return __half2float(__ldg(p)); }
+  static __device__ __forceinline__ float cv(__half v) { return __half2float(v); }
   static __device__ __forceinline__ void st(__half *p, float v) { *p = __float2half_rn(v); }
 };
 template <> struct ftraits<__nv_bfloat16> {
@@ -66,6 +71,7 @@ template <> struct ftraits<__nv_bfloat16> {
   static constexpr int SPB = 24, FACE = 12;
   static constexpr bool WIDE_ONLY = true;
   static __device__ __forceinline__ float ld(const __nv_bfloat16 *p) { return __bfloat162float(__ldg(p)); }
+  static __device__ __forceinline__ float cv(__nv_bfloat16 v) { return __bfloat162float(v); }
   static __device__ __forceinline__ void st(__nv_bfloat16 *p, float v) { *p = __float2bfloat16_rn(v); }
 };
 template <> struct ftraits<half_norm> {
@@ -74,6 +80,7 @@ template <> struct ftraits<half_norm> {
   static constexpr int SPB = 26, FACE = 14;
   static constexpr bool WIDE_ONLY = true;
   static __device__ __forceinline__ float ld(const __half *p) { return __half2float(__ldg(p)); }
+  static __device__ __forceinline__ float cv(__half v) { return __half2float(v); }
   static __device__ __forceinline__ void st(__half *p, float v) { *p = __float2half_rn(v); }
 };
 

@@ -1,8 +1,11 @@
 // qb200_inst.cu -- kernel instantiations and launchers for one storage type
 // and SOALEN.  Compiled once per (QB_FT, QB_S) pair by the build so that the
 // translation units build in parallel.
+#include <cstdint>
+
 #include "qb200_face_kernel.cuh"
 #include "qb200_internal.h"
+#include "qb200_staged_kernel.cuh"
 #if QB_MRHS
 #include "qb200_pair_kernel.cuh"
 #endif
@@ -27,6 +30,17 @@ cudaError_t go(const KArgs<FT> &a, const GeoDev &g, const OpDev<typename ftraits
   const long long n = (long long)g.nxh * g.ny * (MR ? g.nrhs : 1);
   const dim3 grid((unsigned)((n + kThreads - 1) / kThreads), (unsigned)(g.nz * g.nt));
   if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
+  // narrow layouts (a spinor component of a block shorter than a sector) with
+  // VECLEN == SOALEN: every field staged through shared memory in 16-byte
+  // vectors
+  if constexpr (!MR && staged_layout<FT, S>()) {
+    const bool al = (((uintptr_t)a.psi | (uintptr_t)a.out | (uintptr_t)a.gauge) % 16 == 0) &&
+                    (!ACH || (uintptr_t)a.chi % 16 == 0) && (FAM != FAM_CLOVER || (uintptr_t)a.clov % 16 == 0);
+    if (g.V == S && al) {
+      staged_site_kernel<FT, S, COMP12, FAM, ACH><<<grid, kThreads, 0, st>>>(a, g, p);
+      return cudaGetLastError();
+    }
+  }
   // VECLEN known at compile time for the V == S layouts
   if (S >= 4 && g.V == S) site_dslash_kernel<FT, S, COMP12, FAM, ACH, MR, (S >= 4 ? S : 0)><<<grid, kThreads, 0, st>>>(a, g, p);
   else site_dslash_kernel<FT, S, COMP12, FAM, ACH, MR, 0><<<grid, kThreads, 0, st>>>(a, g, p);

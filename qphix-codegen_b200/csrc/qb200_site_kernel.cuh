@@ -98,6 +98,89 @@ __device__ __forceinline__ void do_hop(const KArgs<FT> &a, const GeoDev &g,
   recons<C, MU>(ub, beta, tau, acc);
 }
 
+// A.chi + (i rho g5 chi) into res: the pre-term of the achimbdpsi form
+// (achiResult, dslash_common.cc:1559-1655; rho term :1873-1906)
+template <typename FT, int FAM>
+__device__ __forceinline__ void ach_pre(const KArgs<FT> &a, const OpDev<typename ftraits<FT>::C> &p, long long tile,
+                                        int lane, int V, const cx<typename ftraits<FT>::C> (&ch)[4][3],
+                                        cx<typename ftraits<FT>::C> (&res)[4][3])
+{
+  typedef typename ftraits<FT>::C C;
+  if (FAM == FAM_WILSON) {
+#pragma unroll
+    for (int sp = 0; sp < 4; sp++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) res[sp][c] = mk<C>(p.alpha * ch[sp][c].re, p.alpha * ch[sp][c].im);
+  } else if (FAM == FAM_TM) {
+    // alpha (1 +/- i mu g5) chi, + on the upper spins for plus
+#pragma unroll
+    for (int sp = 0; sp < 4; sp++) {
+      const C m = (((sp < 2) == (p.isPlus != 0)) ? (C)1 : (C)-1) * p.mu;
+#pragma unroll
+      for (int c = 0; c < 3; c++)
+        res[sp][c] = mk<C>(p.alpha * fma(-m, ch[sp][c].im, ch[sp][c].re),
+                           p.alpha * fma(m, ch[sp][c].re, ch[sp][c].im));
+    }
+  } else {
+    const long long cbase = tile * ((FAM == FAM_CLOVER ? 72LL : 144LL) * V) + lane;
+#pragma unroll
+    for (int blk = 0; blk < 2; blk++) {
+      if (FAM == FAM_CLOVER) clover_block<FT, false>(a.clov, cbase, V, blk, ch, res);
+      else full_clover_block<FT, false>(a.clov, cbase, V, blk, ch, res);
+    }
+#pragma unroll
+    for (int sp = 0; sp < 4; sp++) {
+      const C r = (((p.isPlus != 0) != (sp >= 2)) ? (C)1 : (C)-1) * p.rho;
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        res[sp][c].re = fma(-r, ch[sp][c].im, res[sp][c].re);
+        res[sp][c].im = fma(r, ch[sp][c].re, res[sp][c].im);
+      }
+    }
+  }
+}
+
+// res = post-term(acc): clover / full clover / inverse twisted mass / copy
+// (dslash_plain_body, dslash_common.cc:1796-1826)
+template <typename FT, int FAM>
+__device__ __forceinline__ void plain_post(const KArgs<FT> &a, const OpDev<typename ftraits<FT>::C> &p,
+                                           long long tile, int lane, int V,
+                                           const cx<typename ftraits<FT>::C> (&acc)[4][3],
+                                           cx<typename ftraits<FT>::C> (&res)[4][3])
+{
+  typedef typename ftraits<FT>::C C;
+  if (FAM == FAM_CLOVER || FAM == FAM_TMCLOV) {
+    const long long cbase = tile * ((FAM == FAM_CLOVER ? 72LL : 144LL) * V) + lane;
+#pragma unroll
+    for (int blk = 0; blk < 2; blk++) {
+      if (FAM == FAM_CLOVER) clover_block<FT, false>(a.clov, cbase, V, blk, acc, res);
+      else full_clover_block<FT, false>(a.clov, cbase, V, blk, acc, res);
+    }
+  } else if (FAM == FAM_TM) {
+    inv_twisted<C, false>(acc, p.isPlus, p.mu, p.muinv, res);
+  } else {
+#pragma unroll
+    for (int sp = 0; sp < 4; sp++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) res[sp][c] = acc[sp][c];
+  }
+}
+
+template <typename FT, int S, bool COMP12, bool MR, int VV>
+__device__ __forceinline__ void all_hops(const KArgs<FT> &a, const GeoDev &g, const OpDev<typename ftraits<FT>::C> &p,
+                                         const Site &s, long long obase, long long ue, int le, long long gbase,
+                                         cx<typename ftraits<FT>::C> (&acc)[4][3])
+{
+  do_hop<FT, S, COMP12, 0, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
+  do_hop<FT, S, COMP12, 1, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
+  do_hop<FT, S, COMP12, 2, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
+  do_hop<FT, S, COMP12, 3, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
+  do_hop<FT, S, COMP12, 4, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
+  do_hop<FT, S, COMP12, 5, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
+  do_hop<FT, S, COMP12, 6, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
+  do_hop<FT, S, COMP12, 7, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
+}
+
 // The operator at one output site s (and right-hand side rhs of the
 // multi-RHS layout when MR).
 template <typename FT, int S, bool COMP12, int FAM, bool ACH, bool MR, int VV>
@@ -117,87 +200,26 @@ __device__ __forceinline__ void site_body(const KArgs<FT> &a, const GeoDev &g,
   const int cs = S * nr;
 
   cx<C> res[4][3];
-  cx<C> acc[4][3];
 #pragma unroll
   for (int sp = 0; sp < 4; sp++)
 #pragma unroll
     for (int c = 0; c < 3; c++) res[sp][c] = mk<C>(0, 0);
 
   if (ACH) {
-    // A.chi first (achiResult, dslash_common.cc:1559-1655), then the hops are
-    // subtracted (beta already negated by the host)
+    // A.chi first, then the hops are subtracted (beta already negated by the host)
     cx<C> ch[4][3];
     if (MR) load_spinor_rs<FT>(a.chi, obase, cs, ch);
     else load_spinor<FT, S>(a.chi, obase, ch);
-    if (FAM == FAM_WILSON) {
-#pragma unroll
-      for (int sp = 0; sp < 4; sp++)
-#pragma unroll
-        for (int c = 0; c < 3; c++) res[sp][c] = mk<C>(p.alpha * ch[sp][c].re, p.alpha * ch[sp][c].im);
-    } else if (FAM == FAM_TM) {
-      // alpha (1 +/- i mu g5) chi, + on the upper spins for plus
-#pragma unroll
-      for (int sp = 0; sp < 4; sp++) {
-        const C m = (((sp < 2) == (p.isPlus != 0)) ? (C)1 : (C)-1) * p.mu;
-#pragma unroll
-        for (int c = 0; c < 3; c++)
-          res[sp][c] = mk<C>(p.alpha * fma(-m, ch[sp][c].im, ch[sp][c].re),
-                             p.alpha * fma(m, ch[sp][c].re, ch[sp][c].im));
-      }
-    } else {
-      const long long cbase = tile * ((FAM == FAM_CLOVER ? 72LL : 144LL) * V) + lane;
-#pragma unroll
-      for (int blk = 0; blk < 2; blk++) {
-        if (FAM == FAM_CLOVER) clover_block<FT, false>(a.clov, cbase, V, blk, ch, res);
-        else full_clover_block<FT, false>(a.clov, cbase, V, blk, ch, res);
-      }
-      // + i rho g5 chi for plus (dslash_common.cc:1873-1906)
-#pragma unroll
-      for (int sp = 0; sp < 4; sp++) {
-        const C r = (((p.isPlus != 0) != (sp >= 2)) ? (C)1 : (C)-1) * p.rho;
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-          res[sp][c].re = fma(-r, ch[sp][c].im, res[sp][c].re);
-          res[sp][c].im = fma(r, ch[sp][c].re, res[sp][c].im);
-        }
-      }
-    }
-    do_hop<FT, S, COMP12, 0, MR, VV>(a, g, p, s, obase, ue, le, gbase, res);
-    do_hop<FT, S, COMP12, 1, MR, VV>(a, g, p, s, obase, ue, le, gbase, res);
-    do_hop<FT, S, COMP12, 2, MR, VV>(a, g, p, s, obase, ue, le, gbase, res);
-    do_hop<FT, S, COMP12, 3, MR, VV>(a, g, p, s, obase, ue, le, gbase, res);
-    do_hop<FT, S, COMP12, 4, MR, VV>(a, g, p, s, obase, ue, le, gbase, res);
-    do_hop<FT, S, COMP12, 5, MR, VV>(a, g, p, s, obase, ue, le, gbase, res);
-    do_hop<FT, S, COMP12, 6, MR, VV>(a, g, p, s, obase, ue, le, gbase, res);
-    do_hop<FT, S, COMP12, 7, MR, VV>(a, g, p, s, obase, ue, le, gbase, res);
+    ach_pre<FT, FAM>(a, p, tile, lane, V, ch, res);
+    all_hops<FT, S, COMP12, MR, VV>(a, g, p, s, obase, ue, le, gbase, res);
   } else {
+    cx<C> acc[4][3];
 #pragma unroll
     for (int sp = 0; sp < 4; sp++)
 #pragma unroll
       for (int c = 0; c < 3; c++) acc[sp][c] = mk<C>(0, 0);
-    do_hop<FT, S, COMP12, 0, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
-    do_hop<FT, S, COMP12, 1, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
-    do_hop<FT, S, COMP12, 2, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
-    do_hop<FT, S, COMP12, 3, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
-    do_hop<FT, S, COMP12, 4, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
-    do_hop<FT, S, COMP12, 5, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
-    do_hop<FT, S, COMP12, 6, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
-    do_hop<FT, S, COMP12, 7, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
-    if (FAM == FAM_CLOVER || FAM == FAM_TMCLOV) {
-      const long long cbase = tile * ((FAM == FAM_CLOVER ? 72LL : 144LL) * V) + lane;
-#pragma unroll
-      for (int blk = 0; blk < 2; blk++) {
-        if (FAM == FAM_CLOVER) clover_block<FT, false>(a.clov, cbase, V, blk, acc, res);
-        else full_clover_block<FT, false>(a.clov, cbase, V, blk, acc, res);
-      }
-    } else if (FAM == FAM_TM) {
-      inv_twisted<C, false>(acc, p.isPlus, p.mu, p.muinv, res);
-    } else {
-#pragma unroll
-      for (int sp = 0; sp < 4; sp++)
-#pragma unroll
-        for (int c = 0; c < 3; c++) res[sp][c] = acc[sp][c];
-    }
+    all_hops<FT, S, COMP12, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
+    plain_post<FT, FAM>(a, p, tile, lane, V, acc, res);
   }
   if (MR) store_spinor_rs<FT>(a.out, obase, cs, res);
   else store_spinor<FT, S>(a.out, obase, res);

@@ -153,6 +153,13 @@ SIGNATURES.update({
 INFO.update({
     "qb200_tune_cache_clear": ([], None),
 })
+SIGNATURES.update({
+    "qb200_pack_spinor": [_LAT, _I, _P, _P, _P],
+    "qb200_unpack_spinor": [_LAT, _I, _P, _P, _P],
+    "qb200_pack_gauge": [_LAT, _I, _I, _P, _I, _I, _P, _P],
+    "qb200_pack_clover": [_LAT, _I, _P, _P, _P],
+    "qb200_pack_full_clover": [_LAT, _I, _P, _P, _P],
+})
 INFO.update({
     "qb200_hop_force_elems": ([_LAT], _LL),
 })

@@ -38,6 +38,7 @@ LAYOUTS = [
     (1, 1, F32), (2, 2, F32), (4, 4, F32), (4, 16, F32), (8, 8, F32), (16, 16, F32),
     (4, 8, F64), (8, 8, F64), (4, 16, F16), (8, 8, F16), (16, 16, F16),
     (4, 8, F16N), (16, 16, F16N), (8, 16, BF16), (16, 16, BF16),
+    (4, 4, F64), (4, 4, F16), (8, 8, F16N), (4, 4, BF16),
 ]
 
 
@@ -83,3 +84,21 @@ def test_padding_and_time_edges(cuda):
         a = _run_gpu(g, f, fam, "dslash", 1, 1, pp, cuda)
         b = _run_oracle(g, f, fam, "dslash", 1, 1, pp)
         assert H.site_rel_err(g, a, b) < TOL[F32]
+
+
+@pytest.mark.parametrize("dims,soa,ft", [((8, 6, 4, 4), 4, F32), ((24, 6, 4, 4), 4, F32), ((16, 6, 4, 4), 8, F64),
+                                         ((24, 10, 4, 4), 4, F16N), ((48, 2, 4, 4), 8, BF16)])
+def test_staged_layouts_ragged_planes(cuda, dims, soa, ft):
+    """SOALEN 4/8 with VECLEN == SOALEN (the shared-memory staged kernel),
+    including planes whose site count is not a multiple of 32 (idle lanes),
+    padding, and the skipped t hops of a communicated boundary."""
+    for pad, acc in (((0, 0), None), ((3, 5), [1, 1, 1, 1, 1, 1, 0, 0])):
+        g = Geometry(*dims, soalen=soa, veclen=soa, ftype=ft, compress12=True, t_boundary=-1.0,
+                     pad_xy=pad[0], pad_xyz=pad[1])
+        f = H.make_fields(g, cb=1, seed=140)
+        for fam in H.FAMILIES:
+            for kernel in H.KERNELS:
+                pp = H.op_params(fam, kernel, tbc_mask=13, accumulate=acc)
+                a = _run_gpu(g, f, fam, kernel, 1, 1, pp, cuda)
+                b = _run_oracle(g, f, fam, kernel, 1, 1, pp)
+                assert H.site_rel_err(g, a, b) < TOL[ft], (fam, kernel, pad)
