@@ -111,6 +111,26 @@ cudaError_t go_unpack(const elem_t<FT> *buf, const elem_t<FT> *gauge, const elem
 template <typename FT, int S, bool COMP12, int FAM, bool ACH>
 cudaError_t go_batch(const BatchDev<FT> &b, bool vfixed, int grid, int block, cudaStream_t st)
 {
+  // narrow layouts: the staged kernel, one warp per 32 sites of a plane
+  if constexpr (staged_layout<FT, S>()) {
+    bool al = vfixed;
+    for (int k = 0; k < b.n && al; k++) {
+      const KArgs<FT> &x = b.it[k].a;
+      al = (((uintptr_t)x.psi | (uintptr_t)x.out | (uintptr_t)x.gauge) % 16 == 0) &&
+           (!ACH || (uintptr_t)x.chi % 16 == 0) && (FAM != FAM_CLOVER || (uintptr_t)x.clov % 16 == 0);
+    }
+    if (al) {
+      BatchDev<FT> bw = b;
+      long long first = 0;
+      for (int k = 0; k < b.n; k++) {
+        bw.it[k].first = first;
+        first += (long long)b.it[k].g.nz * b.it[k].g.nt * ((b.it[k].g.nxh * b.it[k].g.ny + 31) / 32);
+      }
+      bw.total = first;
+      batch_staged_kernel<FT, S, COMP12, FAM, ACH><<<grid, block, 0, st>>>(bw);
+      return cudaGetLastError();
+    }
+  }
   if (S >= 4 && vfixed) batch_dslash_kernel<FT, S, COMP12, FAM, ACH, (S >= 4 ? S : 0)><<<grid, block, 0, st>>>(b);
   else if (S < 4) batch_dslash_kernel<FT, S, COMP12, FAM, ACH, 0><<<grid, block, 0, st>>>(b);
   else return cudaErrorInvalidValue; // SOALEN >= 4 layouts batch only with VECLEN == SOALEN

@@ -80,3 +80,25 @@ def test_batch_rejects_mixed_layouts(cuda):
     probs[1].g = g2
     with pytest.raises(_lib.QB200Error):
         batch.BatchedDslash("wilson", "dslash", 1, probs)()
+
+
+def test_batched_ragged_planes(cuda):
+    """planes whose site count is not a multiple of 32 (the staged batched
+    kernel pads each plane to whole warps)"""
+    global DIMS
+    saved = DIMS
+    try:
+        DIMS = [(24, 6, 4, 4), (8, 6, 4, 4), (16, 8, 4, 4)]
+        for family in ("clover", "tm"):
+            for kernel in H.KERNELS:
+                probs, refs = _problems(F32, 4, family, kernel, True, cuda, seed=320)
+                op = batch.BatchedDslash(family, kernel, 1, probs)
+                for grid, block in ((0, 128), (2, 128), (5, 64)):
+                    for p in probs:
+                        p.out.zero_()
+                    op(grid=grid, block=block)
+                    torch.cuda.synchronize()
+                    for p, r in zip(probs, refs):
+                        assert torch.equal(p.out, r), (family, kernel, grid, block)
+    finally:
+        DIMS = saved
