@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bound of the CPU baseline sample")
     ap.add_argument("--no-extras", action="store_true", help="skip the multi-RHS and solver measurements")
-    ap.add_argument("--only", choices=["mrhs", "force", "batch", "solve"],
+    ap.add_argument("--only", choices=["mrhs", "force", "batch", "solve", "tm"],
                     help="run one secondary measurement alone (on --dims) and print its JSON line")
     return ap.parse_args()
 
@@ -390,6 +390,41 @@ def bench_batch(dev, peak):
     return res
 
 
+def bench_tm(dev, dims=(48, 48, 48, 96)):
+    """Twisted-mass dslash, and twisted-mass clover, at 48^3x96 with FP16
+    spinors scaled by a per-site norm (QB200_F16N; links and clover FP16,
+    12-real links), SOALEN = VECLEN = 8 (nx/2 = 24).  mu = 0.01, kappa = 0.16:
+    alpha = 1/(2 kappa), mu~ = mu/alpha and muinv = alpha/(alpha^2 + mu^2)
+    as the caller passes them.  Algorithmic bytes per site: psi + out
+    (24 halves + 4-byte norm each) + 8 x 12 halves of links = 296 (+ 2 x 144
+    halves of clover for TM clover = 584); flop per site: 1320 + 72 (TM) or
+    1320 + 504 (TM clover, counted as clover)."""
+    from qphix_b200 import fields, layout, ops
+    from qphix_b200.lattice import F16N, Geometry
+    g = Geometry(*dims, soalen=8, veclen=8, ftype=F16N, compress12=True, t_boundary=-1.0)
+    U = fields.random_gauge(g, seed=96, device=dev)
+    gauge = layout.pack_gauge(g, U, 0)
+    del U
+    psi = layout.pack_spinor(g, fields.random_spinor(g, seed=97, device=dev))
+    fcl = layout.pack_full_clover(g, fields.random_full_clover(g, seed=98, device=dev))
+    out = torch.zeros_like(psi)
+    kappa, mu = 0.16, 0.01
+    alpha = 1.0 / (2 * kappa)
+    kw = dict(coeff_s=1.0, coeff_t_f=1.0, coeff_t_b=1.0, mu=mu / alpha, muinv=alpha / (alpha ** 2 + mu ** 2))
+    stream = torch.cuda.current_stream()
+    peak = measured_peak()[0]
+    n = g.vol_cb
+    res = {"lattice": list(dims), "storage": "fp16 + per-site norm", "soalen": 8, "sites_per_cb": n}
+    t = _time(lambda: ops.dslash(g, "tm", "dslash", 1, 0, psi, out, gauge, **kw), 20, stream)
+    res["tm_dslash"] = {"ms": t, "gbs": 296 * n / (t * 1e-3) / 1e9, "frac_of_peak": 296 * n / (t * 1e-3) / 1e9 / peak,
+                        "gflops": 1392 * n / (t * 1e-3) / 1e9, "bytes_per_site": 296}
+    t = _time(lambda: ops.dslash(g, "tm_clover", "dslash", 1, 0, psi, out, gauge, clover=fcl), 20, stream)
+    res["tm_clover_dslash"] = {"ms": t, "gbs": 584 * n / (t * 1e-3) / 1e9,
+                               "frac_of_peak": 584 * n / (t * 1e-3) / 1e9 / peak,
+                               "gflops": FLOP_SITE * n / (t * 1e-3) / 1e9, "bytes_per_site": 584}
+    return res
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -586,6 +621,7 @@ def b200_arm(args, world, rank, local):
         extras["solve"] = bench_solve(dims, dev)
         extras["force"] = bench_force(dev)
         extras["batch"] = bench_batch(dev, peak)
+        extras["tm_fp16n"] = bench_tm(dev)
 
     if rank == 0:
         line = {
@@ -624,6 +660,8 @@ def run_only(args):
         r = bench_force(dev, dims)
     elif args.only == "batch":
         r = bench_batch(dev, measured_peak()[0])
+    elif args.only == "tm":
+        r = bench_tm(dev, dims)
     else:
         r = bench_solve(dims, dev)
     print(json.dumps({"only": args.only, "dims": list(dims), "result": r}))

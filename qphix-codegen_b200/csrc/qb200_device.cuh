@@ -301,6 +301,28 @@ __device__ __forceinline__ void store_spinor_rs(elem_t<FT> *__restrict__ f, long
     }
 }
 
+// third row of a 12-real link: G[2][c] = conj(G[0][c+1] G[1][c+2] -
+// G[0][c+2] G[1][c+1]), in a fixed order of fused multiply-adds (every
+// kernel uses this order, so all give the same bits)
+template <typename C>
+__device__ __forceinline__ void recon_row3(cx<C> (&G)[3][3])
+{
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+    C re = G[0][c1].re * G[1][c2].re;
+    re = fma(-G[0][c1].im, G[1][c2].im, re);
+    re = fma(-G[0][c2].re, G[1][c1].re, re);
+    re = fma(G[0][c2].im, G[1][c1].im, re);
+    C im = G[0][c1].re * G[1][c2].im;
+    im = fma(G[0][c1].im, G[1][c2].re, im);
+    im = fma(-G[0][c2].re, G[1][c1].im, im);
+    im = fma(-G[0][c2].im, G[1][c1].re, im);
+    G[2][c].re = re;
+    G[2][c].im = -im;
+  }
+}
+
 // stored link G (= U^T) of direction D; `base` = tile*(8*R*6*V) + lane
 template <typename FT, bool COMP12, int D>
 __device__ __forceinline__ void load_link(const elem_t<FT> *__restrict__ u, long long base, int V,
@@ -314,19 +336,7 @@ __device__ __forceinline__ void load_link(const elem_t<FT> *__restrict__ u, long
       G[r][c].re = ftraits<FT>::ld(u + base + (long long)(((D * R + r) * 3 + c) * 2 + 0) * V);
       G[r][c].im = ftraits<FT>::ld(u + base + (long long)(((D * R + r) * 3 + c) * 2 + 1) * V);
     }
-  if (COMP12) {
-    // G[2][c] = conj(G[0][c+1] G[1][c+2] - G[0][c+2] G[1][c+1])
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-      const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
-      typename ftraits<FT>::C re = G[0][c1].re * G[1][c2].re - G[0][c1].im * G[1][c2].im
-                                 - G[0][c2].re * G[1][c1].re + G[0][c2].im * G[1][c1].im;
-      typename ftraits<FT>::C im = G[0][c1].re * G[1][c2].im + G[0][c1].im * G[1][c2].re
-                                 - G[0][c2].re * G[1][c1].im - G[0][c2].im * G[1][c1].re;
-      G[2][c].re = re;
-      G[2][c].im = -im;
-    }
-  }
+  if (COMP12) recon_row3(G);
 }
 
 // ---------------------------------------------------------------------

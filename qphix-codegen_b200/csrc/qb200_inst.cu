@@ -2,10 +2,21 @@
 // and SOALEN.  Compiled once per (QB_FT, QB_S) pair by the build so that the
 // translation units build in parallel.
 #include <cstdint>
+#include <type_traits>
 
 #include "qb200_face_kernel.cuh"
 #include "qb200_internal.h"
 #include "qb200_staged_kernel.cuh"
+#include "qb200_site2_kernel.cuh"
+
+// two sites per thread (qb200_site2_kernel.cuh) for the single-RHS operator
+#ifndef QB_SITE2
+#define QB_SITE2 0
+#endif
+// prefer it to the staged kernel on narrow layouts
+#ifndef QB_SITE2_OVER_STAGED
+#define QB_SITE2_OVER_STAGED 0
+#endif
 #if QB_MRHS
 #include "qb200_pair_kernel.cuh"
 #endif
@@ -30,6 +41,19 @@ cudaError_t go(const KArgs<FT> &a, const GeoDev &g, const OpDev<typename ftraits
   const long long n = (long long)g.nxh * g.ny * (MR ? g.nrhs : 1);
   const dim3 grid((unsigned)((n + kThreads - 1) / kThreads), (unsigned)(g.nz * g.nt));
   if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
+  // two sites per thread in packed FP32x2 arithmetic
+  if constexpr (QB_SITE2 && !MR && S >= 2 && !std::is_same<FT, double>::value &&
+                (QB_SITE2_OVER_STAGED || !staged_layout<FT, S>())) {
+    const bool al = (((uintptr_t)a.psi | (uintptr_t)a.out | (uintptr_t)a.gauge) % 8 == 0) &&
+                    (!ACH || (uintptr_t)a.chi % 8 == 0) && (FAM == FAM_WILSON || FAM == FAM_TM ||
+                                                              (uintptr_t)a.clov % 8 == 0);
+    if (al && (p.acc_mask & 3u) == 3u) {
+      const dim3 g2((unsigned)(((long long)(g.nxh / 2) * g.ny + kThreads - 1) / kThreads), (unsigned)(g.nz * g.nt));
+      if (S >= 4 && g.V == S) site2_dslash_kernel<FT, S, COMP12, FAM, ACH, (S >= 4 ? S : 0)><<<g2, kThreads, 0, st>>>(a, g, p);
+      else site2_dslash_kernel<FT, S, COMP12, FAM, ACH, 0><<<g2, kThreads, 0, st>>>(a, g, p);
+      return cudaGetLastError();
+    }
+  }
   // narrow layouts (a spinor component of a block shorter than a sector) with
   // VECLEN == SOALEN: every field staged through shared memory in 16-byte
   // vectors

@@ -229,8 +229,13 @@ __device__ __forceinline__ void site_body(const KArgs<FT> &a, const GeoDev &g,
 // right-hand sides).  MR: multi-RHS layout, one thread per (site, right-hand
 // side) with the right-hand side fastest, so the nrhs threads of a site share
 // each link and clover load.
+// minimum resident blocks per SM the register allocation must allow
+#ifndef QB_SITE_MINB
+#define QB_SITE_MINB 1
+#endif
+
 template <typename FT, int S, bool COMP12, int FAM, bool ACH, bool MR, int VV>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, QB_SITE_MINB)
     site_dslash_kernel(const KArgs<FT> a, const GeoDev g, const OpDev<typename ftraits<FT>::C> p)
 {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;

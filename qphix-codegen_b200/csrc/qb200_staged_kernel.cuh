@@ -40,9 +40,14 @@ template <typename FT, int S> struct Stage {
   static constexpr int BUF = G * (SP > CL ? (SP > LK18 ? SP : LK18) : (CL > LK18 ? CL : LK18));
 };
 
+// largest component piece (bytes) that is staged
+#ifndef QB_STAGE_MAXPIECE
+#define QB_STAGE_MAXPIECE 16
+#endif
+
 template <typename FT, int S> constexpr bool staged_layout()
 {
-  return (S == 4 || S == 8) && S * (int)sizeof(elem_t<FT>) < 32;
+  return (S == 4 || S == 8) && S * (int)sizeof(elem_t<FT>) <= QB_STAGE_MAXPIECE;
 }
 
 // Copy, for every group of the warp, the BYTES bytes that start at element
@@ -158,18 +163,7 @@ __device__ __forceinline__ void load_link_sm(const unsigned char *grp, int lane,
       G[r][c].re = sm_ld<FT, S>(grp, (r * 3 + c) * 2 + 0, lane);
       G[r][c].im = sm_ld<FT, S>(grp, (r * 3 + c) * 2 + 1, lane);
     }
-  if (COMP12) {
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-      const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
-      C re = G[0][c1].re * G[1][c2].re - G[0][c1].im * G[1][c2].im - G[0][c2].re * G[1][c1].re +
-             G[0][c2].im * G[1][c1].im;
-      C im = G[0][c1].re * G[1][c2].im + G[0][c1].im * G[1][c2].re - G[0][c2].re * G[1][c1].im -
-             G[0][c2].im * G[1][c1].re;
-      G[2][c].re = re;
-      G[2][c].im = -im;
-    }
-  }
+  if (COMP12) recon_row3(G);
 }
 
 // clover_block from a staged CloverBlock half (the same operations)
