@@ -1,0 +1,228 @@
+// qb200_async_kernel.cuh -- the single-RHS dslash with the neighbour spinors
+// and links of the next hop in flight while the current hop computes.
+//
+// The thread-per-site kernel waits on global loads (long-scoreboard stalls)
+// with about 20 warps per SM: each hop's 24 spinor and 12-18 link loads are
+// issued only when the hop starts.  Here a warp copies, with cp.async, the
+// blocks its 32 sites need for hop D+1 (the neighbour spinor blocks, or its
+// own blocks of psi for the x hops, and the direction-(D+1) slab of its link
+// tiles) into one of two shared-memory buffers while it computes hop D from
+// the other, so the copies cost no registers and overlap the arithmetic.
+// The per-site reads from shared memory, the x-neighbour handling and the
+// clover / chi / result staging are those of qb200_staged_kernel.cuh; the
+// arithmetic is that of site_body, operation for operation.
+// Layouts with VECLEN == SOALEN in {4, 8, 16}, 32- and 16-bit storage.
+#pragma once
+
+#include "qb200_staged_kernel.cuh"
+
+namespace qb200 {
+
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src)
+{
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait()
+{
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// stage_in with asynchronous copies (completion: cp_async_wait + __syncwarp)
+template <typename FT, int S, int BYTES, int STRIDE>
+__device__ __forceinline__ void stage_in_async(const elem_t<FT> *__restrict__ f, long long start, unsigned char *buf,
+                                               int ln)
+{
+  static_assert(BYTES % 16 == 0 && STRIDE % 16 == 0, "staged pieces are whole 16-byte vectors");
+  constexpr int CH = BYTES / 16, N = CH * Stage<FT, S>::G, ROUNDS = (N + 31) / 32;
+  const uint4 *base = reinterpret_cast<const uint4 *>(f);
+  const unsigned v16 = (unsigned)(start * (long long)sizeof(elem_t<FT>) / 16);
+#pragma unroll
+  for (int r = 0; r < ROUNDS; r++) {
+    const int j = ln + 32 * r;
+    const int gi = (j < N ? j : 0) / CH;
+    const unsigned st = __shfl_sync(0xffffffffu, v16, gi * S);
+    if (j < N) cp_async16(buf + gi * STRIDE + (j - gi * CH) * 16, base + st + (j - gi * CH));
+  }
+}
+
+template <typename FT, int S, bool COMP12> struct AsyncCfg {
+  typedef Stage<FT, S> St;
+  static constexpr int R = COMP12 ? 2 : 3;
+  static constexpr int SPB = St::SPB * S * (int)sizeof(elem_t<FT>);  // spinor block bytes
+  static constexpr int LKB = R * 6 * S * (int)sizeof(elem_t<FT>);    // link slab bytes
+  static constexpr int LKS = St::stride(R * 6);
+  static constexpr int HOP = St::G * (St::SP + LKS);                 // one hop's staged bytes
+  static constexpr int BUF = (2 * HOP > St::G * St::CL) ? 2 * HOP : St::G * St::CL;
+};
+
+template <typename FT, int S> constexpr bool async_layout()
+{
+  return (S == 4 || S == 8 || S == 16) && sizeof(elem_t<FT>) <= 4;
+}
+
+// issue the copies of hop D into buf
+template <typename FT, int S, bool COMP12, int D>
+__device__ __forceinline__ void prefetch_hop(const KArgs<FT> &a, const GeoDev &g, const Site &s, long long obase,
+                                             const WarpCtx &w, unsigned char *buf)
+{
+  typedef AsyncCfg<FT, S, COMP12> A;
+  typedef Stage<FT, S> St;
+  bool cross;
+  const long long nbase = obase + neighbour_offset<S, D>(g, s, (long long)St::SPB * S, 1, &cross);
+  stage_in_async<FT, S, A::SPB, St::SP>(a.psi, D < 2 ? w.own : nbase - w.lane, buf, w.ln);
+  stage_in_async<FT, S, A::LKB, A::LKS>(a.gauge, w.tile * (8LL * A::R * 6 * S) + (long long)D * A::R * 6 * S,
+                                        buf + St::G * St::SP, w.ln);
+}
+
+// hop D from the staged copies in buf (the operations of do_hop)
+template <typename FT, int S, bool COMP12, int D>
+__device__ __forceinline__ void compute_hop(const KArgs<FT> &a, const GeoDev &g, const OpDev<comp_t<FT>> &p,
+                                            const Site &s, long long obase, const WarpCtx &w,
+                                            const unsigned char *buf, cx<comp_t<FT>> (&acc)[4][3])
+{
+  typedef comp_t<FT> C;
+  typedef AsyncCfg<FT, S, COMP12> A;
+  typedef Stage<FT, S> St;
+  constexpr int MU = D / 2;
+  constexpr bool FWD = (D & 1) != 0;
+  bool cross;
+  const long long nbase = obase + neighbour_offset<S, D>(g, s, (long long)St::SPB * S, 1, &cross);
+  if (cross && !((p.acc_mask >> D) & 1u)) return;
+  cx<C> psi[4][3], G[3][3];
+  if (MU == 0) {
+    const long long nb = nbase / (St::SPB * S);
+    const int nl = (int)(nbase - nb * (St::SPB * S));
+    const long long gi = nb - w.blk0;
+    if (gi >= 0 && gi < St::G) load_spinor_sm<FT, S>(buf + gi * St::SP, nl, psi);
+    else load_spinor<FT, S>(a.psi, nbase, psi);
+  } else {
+    load_spinor_sm<FT, S>(buf + (w.ln / S) * St::SP, w.lane, psi);
+  }
+  load_link_sm<FT, S, COMP12>(buf + St::G * St::SP + (w.ln / S) * A::LKS, w.lane, G);
+  C beta = p.beta[D];
+  if (D == 6 && s.t == 0 && p.t_edge_lo) beta *= p.tbound;
+  if (D == 7 && s.t == g.nt - 1 && p.t_edge_hi) beta *= p.tbound;
+  cx<C> b[2][3], ub[2][3];
+  const C sigma = p.isPlus ? (C)1 : (C)-1;
+  project<C, D>(psi, sigma, b);
+  mult_link<C, !FWD>(G, b, ub);
+  if ((p.tbc_mask >> MU) & 1u) {
+    const C pr = p.tbc[MU][0];
+    const C pi = FWD ? p.tbc[MU][1] : -p.tbc[MU][1];
+    apply_phase<C>(ub, pr, pi);
+  }
+  const C tau = ((p.isPlus != 0) != FWD) ? (C)1 : (C)-1;
+  recons<C, MU>(ub, beta, tau, acc);
+}
+
+// one pipeline step: issue hop D+1, wait for hop D, compute hop D
+template <typename FT, int S, bool COMP12, int D>
+__device__ __forceinline__ void pipe_step(const KArgs<FT> &a, const GeoDev &g, const OpDev<comp_t<FT>> &p,
+                                          const Site &s, long long obase, const WarpCtx &w,
+                                          cx<comp_t<FT>> (&acc)[4][3])
+{
+  typedef AsyncCfg<FT, S, COMP12> A;
+  if (D < 7) {
+    prefetch_hop<FT, S, COMP12, (D < 7 ? D + 1 : 7)>(a, g, s, obase, w, w.buf + ((D + 1) & 1) * A::HOP);
+    cp_async_commit();
+    cp_async_wait<1>();
+  } else {
+    cp_async_wait<0>();
+  }
+  __syncwarp();
+  compute_hop<FT, S, COMP12, D>(a, g, p, s, obase, w, w.buf + (D & 1) * A::HOP, acc);
+  __syncwarp();
+}
+
+template <typename FT, int S, bool COMP12>
+__device__ __forceinline__ void async_hops(const KArgs<FT> &a, const GeoDev &g, const OpDev<comp_t<FT>> &p,
+                                           const Site &s, long long obase, const WarpCtx &w,
+                                           cx<comp_t<FT>> (&acc)[4][3])
+{
+  prefetch_hop<FT, S, COMP12, 0>(a, g, s, obase, w, w.buf);
+  cp_async_commit();
+  pipe_step<FT, S, COMP12, 0>(a, g, p, s, obase, w, acc);
+  pipe_step<FT, S, COMP12, 1>(a, g, p, s, obase, w, acc);
+  pipe_step<FT, S, COMP12, 2>(a, g, p, s, obase, w, acc);
+  pipe_step<FT, S, COMP12, 3>(a, g, p, s, obase, w, acc);
+  pipe_step<FT, S, COMP12, 4>(a, g, p, s, obase, w, acc);
+  pipe_step<FT, S, COMP12, 5>(a, g, p, s, obase, w, acc);
+  pipe_step<FT, S, COMP12, 6>(a, g, p, s, obase, w, acc);
+  pipe_step<FT, S, COMP12, 7>(a, g, p, s, obase, w, acc);
+}
+
+// Grid as site_dslash_kernel (blockIdx.y = the (z, t) plane), blocks of 128
+// threads.  Threads past the plane's last site take part in the warp's
+// copies (on a clamped site) and store nothing.  Needs 16-byte aligned fields
+// smaller than 32 GiB.
+template <typename FT, int S, bool COMP12, int FAM, bool ACH>
+__global__ void __launch_bounds__(128, 4)
+    async_site_kernel(const KArgs<FT> a, const GeoDev g, const OpDev<comp_t<FT>> p)
+{
+  typedef comp_t<FT> C;
+  typedef Stage<FT, S> St;
+  typedef AsyncCfg<FT, S, COMP12> A;
+  __shared__ __align__(16) unsigned char smem[4][A::BUF];
+  const int nplane = g.nxh * g.ny;
+  const int q0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = q0 < nplane;
+  const int q = active ? q0 : nplane - 1;
+  Site s;
+  s.z = blockIdx.y % g.nz;
+  s.t = blockIdx.y / g.nz;
+  s.y = q / g.nxh;
+  s.xcb = q - s.y * g.nxh;
+  s.par = (s.y + s.z + s.t + p.cb) & 1;
+  WarpCtx w;
+  w.buf = smem[threadIdx.x >> 5];
+  w.ln = threadIdx.x & 31;
+  w.tile = tile_of<S>(g, s, &w.lane);
+  const long long obase = spinor_base<FT, S>(g, s);
+  w.blk = obase / (St::SPB * S);
+  w.own = w.blk * (St::SPB * S);
+  w.blk0 = __shfl_sync(0xffffffffu, w.blk, 0);
+
+  cx<C> res[4][3];
+#pragma unroll
+  for (int sp = 0; sp < 4; sp++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) res[sp][c] = mk<C>(0, 0);
+  if (ACH) {
+    cx<C> ch[4][3];
+    stage_in<FT, S, A::SPB, St::SP>(a.chi, w.own, w.buf, w.ln);
+    __syncwarp();
+    load_spinor_sm<FT, S>(w.buf + (w.ln / S) * St::SP, w.lane, ch);
+    __syncwarp();
+    if (FAM == FAM_CLOVER) {
+      staged_clover<FT, S>(a, w, ch, res);
+#pragma unroll
+      for (int sp = 0; sp < 4; sp++) {
+        const C r = (((p.isPlus != 0) != (sp >= 2)) ? (C)1 : (C)-1) * p.rho;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          res[sp][c].re = fma(-r, ch[sp][c].im, res[sp][c].re);
+          res[sp][c].im = fma(r, ch[sp][c].re, res[sp][c].im);
+        }
+      }
+    } else {
+      ach_pre<FT, FAM>(a, p, w.tile, w.lane, S, ch, res);
+    }
+    async_hops<FT, S, COMP12>(a, g, p, s, obase, w, res);
+  } else {
+    cx<C> acc[4][3];
+#pragma unroll
+    for (int sp = 0; sp < 4; sp++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) acc[sp][c] = mk<C>(0, 0);
+    async_hops<FT, S, COMP12>(a, g, p, s, obase, w, acc);
+    if (FAM == FAM_CLOVER) staged_clover<FT, S>(a, w, acc, res);
+    else plain_post<FT, FAM>(a, p, w.tile, w.lane, S, acc, res);
+  }
+  store_spinor_sm<FT, S>(w.buf + (w.ln / S) * St::SP, w.lane, res);
+  __syncwarp();
+  stage_out<FT, S, A::SPB, St::SP>(a.out, w.own, w.buf, w.ln, active);
+}
+
+} // namespace qb200

@@ -8,6 +8,12 @@
 #include "qb200_internal.h"
 #include "qb200_staged_kernel.cuh"
 #include "qb200_site2_kernel.cuh"
+#include "qb200_async_kernel.cuh"
+
+// the single-RHS operator with the next hop's copies in flight (cp.async)
+#ifndef QB_ASYNC
+#define QB_ASYNC 1
+#endif
 
 // two sites per thread (qb200_site2_kernel.cuh) for the single-RHS operator
 #ifndef QB_SITE2
@@ -41,6 +47,14 @@ cudaError_t go(const KArgs<FT> &a, const GeoDev &g, const OpDev<typename ftraits
   const long long n = (long long)g.nxh * g.ny * (MR ? g.nrhs : 1);
   const dim3 grid((unsigned)((n + kThreads - 1) / kThreads), (unsigned)(g.nz * g.nt));
   if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
+  if constexpr (QB_ASYNC && !MR && async_layout<FT, S>()) {
+    const bool al = (((uintptr_t)a.psi | (uintptr_t)a.out | (uintptr_t)a.gauge) % 16 == 0) &&
+                    (!ACH || (uintptr_t)a.chi % 16 == 0) && (FAM != FAM_CLOVER || (uintptr_t)a.clov % 16 == 0);
+    if (g.V == S && al) {
+      async_site_kernel<FT, S, COMP12, FAM, ACH><<<grid, kThreads, 0, st>>>(a, g, p);
+      return cudaGetLastError();
+    }
+  }
   // two sites per thread in packed FP32x2 arithmetic
   if constexpr (QB_SITE2 && !MR && S >= 2 && !std::is_same<FT, double>::value &&
                 (QB_SITE2_OVER_STAGED || !staged_layout<FT, S>())) {
