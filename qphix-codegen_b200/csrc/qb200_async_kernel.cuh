@@ -153,30 +153,26 @@ __device__ __forceinline__ void async_hops(const KArgs<FT> &a, const GeoDev &g, 
   pipe_step<FT, S, COMP12, 7>(a, g, p, s, obase, w, acc);
 }
 
-// Grid as site_dslash_kernel (blockIdx.y = the (z, t) plane), blocks of 128
-// threads.  Threads past the plane's last site take part in the warp's
-// copies (on a clamped site) and store nothing.  Needs 16-byte aligned fields
-// smaller than 32 GiB.
+// The operator at site q0 (this lane's) of plane (z, t), all 32 lanes of a
+// warp together; buf is the warp's AsyncCfg::BUF bytes of shared memory.
 template <typename FT, int S, bool COMP12, int FAM, bool ACH>
-__global__ void __launch_bounds__(128, 4)
-    async_site_kernel(const KArgs<FT> a, const GeoDev g, const OpDev<comp_t<FT>> p)
+__device__ __forceinline__ void async_body(const KArgs<FT> &a, const GeoDev &g, const OpDev<comp_t<FT>> &p, int z,
+                                           int t, int q0, unsigned char *buf)
 {
   typedef comp_t<FT> C;
   typedef Stage<FT, S> St;
   typedef AsyncCfg<FT, S, COMP12> A;
-  __shared__ __align__(16) unsigned char smem[4][A::BUF];
   const int nplane = g.nxh * g.ny;
-  const int q0 = blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = q0 < nplane;
   const int q = active ? q0 : nplane - 1;
   Site s;
-  s.z = blockIdx.y % g.nz;
-  s.t = blockIdx.y / g.nz;
+  s.z = z;
+  s.t = t;
   s.y = q / g.nxh;
   s.xcb = q - s.y * g.nxh;
   s.par = (s.y + s.z + s.t + p.cb) & 1;
   WarpCtx w;
-  w.buf = smem[threadIdx.x >> 5];
+  w.buf = buf;
   w.ln = threadIdx.x & 31;
   w.tile = tile_of<S>(g, s, &w.lane);
   const long long obase = spinor_base<FT, S>(g, s);
@@ -223,6 +219,40 @@ __global__ void __launch_bounds__(128, 4)
   store_spinor_sm<FT, S>(w.buf + (w.ln / S) * St::SP, w.lane, res);
   __syncwarp();
   stage_out<FT, S, A::SPB, St::SP>(a.out, w.own, w.buf, w.ln, active);
+  __syncwarp();
+}
+
+// Grid as site_dslash_kernel (blockIdx.y = the (z, t) plane), blocks of 128
+// threads.  Threads past the plane's last site take part in the warp's
+// copies (on a clamped site) and store nothing.  Needs 16-byte aligned fields
+// smaller than 32 GiB.
+template <typename FT, int S, bool COMP12, int FAM, bool ACH>
+__global__ void __launch_bounds__(128, 4)
+    async_site_kernel(const KArgs<FT> a, const GeoDev g, const OpDev<comp_t<FT>> p)
+{
+  __shared__ __align__(16) unsigned char smem[4][AsyncCfg<FT, S, COMP12>::BUF];
+  async_body<FT, S, COMP12, FAM, ACH>(a, g, p, blockIdx.y % g.nz, blockIdx.y / g.nz,
+                                      blockIdx.x * blockDim.x + threadIdx.x, smem[threadIdx.x >> 5]);
+}
+
+// Batched form (see batch_staged_kernel): work unit = one warp's 32 sites of
+// one plane of one item, b.it[k].first and b.total in such warps.
+template <typename FT, int S, bool COMP12, int FAM, bool ACH>
+__global__ void __launch_bounds__(128, 3) batch_async_kernel(const __grid_constant__ BatchDev<FT> b)
+{
+  __shared__ __align__(16) unsigned char smem[4][AsyncCfg<FT, S, COMP12>::BUF];
+  const long long stride = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long u = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < b.total; u += stride) {
+    int k = 0;
+    while (k + 1 < b.n && u >= b.it[k + 1].first) k++;
+    const BatchItem<FT> &it = b.it[k];
+    const int wpp = (it.g.nxh * it.g.ny + 31) >> 5;
+    const long long loc = u - it.first;
+    const int plane = (int)(loc / wpp);
+    const int wi = (int)(loc - (long long)plane * wpp);
+    async_body<FT, S, COMP12, FAM, ACH>(it.a, it.g, it.p, plane % it.g.nz, plane / it.g.nz,
+                                        wi * 32 + (threadIdx.x & 31), smem[threadIdx.x >> 5]);
+  }
 }
 
 } // namespace qb200

@@ -149,8 +149,9 @@ cudaError_t go_unpack(const elem_t<FT> *buf, const elem_t<FT> *gauge, const elem
 template <typename FT, int S, bool COMP12, int FAM, bool ACH>
 cudaError_t go_batch(const BatchDev<FT> &b, bool vfixed, int grid, int block, cudaStream_t st)
 {
-  // narrow layouts: the staged kernel, one warp per 32 sites of a plane
-  if constexpr (staged_layout<FT, S>()) {
+  // async-staged (V == S, S >= 4, 32- or 16-bit) or staged (narrow) kernel,
+  // one warp per 32 sites of a plane
+  if constexpr ((QB_ASYNC && async_layout<FT, S>()) || staged_layout<FT, S>()) {
     bool al = vfixed;
     for (int k = 0; k < b.n && al; k++) {
       const KArgs<FT> &x = b.it[k].a;
@@ -165,7 +166,9 @@ cudaError_t go_batch(const BatchDev<FT> &b, bool vfixed, int grid, int block, cu
         first += (long long)b.it[k].g.nz * b.it[k].g.nt * ((b.it[k].g.nxh * b.it[k].g.ny + 31) / 32);
       }
       bw.total = first;
-      batch_staged_kernel<FT, S, COMP12, FAM, ACH><<<grid, block, 0, st>>>(bw);
+      if constexpr (QB_ASYNC && async_layout<FT, S>())
+        batch_async_kernel<FT, S, COMP12, FAM, ACH><<<grid, block, 0, st>>>(bw);
+      else batch_staged_kernel<FT, S, COMP12, FAM, ACH><<<grid, block, 0, st>>>(bw);
       return cudaGetLastError();
     }
   }

@@ -14,10 +14,14 @@ from qphix_b200.solver import EvenOddOperator
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("soa,vec,ft,nrhs", [(4, 16, F32, 4), (8, 8, F32, 8), (16, 16, F16, 16), (8, 8, F16, 2),
-                                             (4, 4, F32, 1), (16, 16, F32, 2), (4, 8, F16, 8)])
-def test_mrhs_dslash_matches_single(cuda, soa, vec, ft, nrhs):
-    g = Geometry(max(8, 2 * soa), 8, 4, 4, soalen=soa, veclen=vec, ftype=ft, compress12=True, t_boundary=-1.0)
+@pytest.mark.parametrize("soa,vec,ft,nrhs,ny", [
+    (4, 16, F32, 4, 8), (8, 8, F32, 8, 8), (16, 16, F16, 16, 8), (8, 8, F16, 2, 8), (4, 4, F32, 1, 8),
+    (16, 16, F32, 2, 8), (4, 8, F16, 8, 8),
+    # FP16 with VECLEN == SOALEN: the kernel with the next hop's copies in flight,
+    # one to four blocks per warp, and planes that end inside a warp (ny = 6)
+    (4, 4, F16, 4, 8), (8, 8, F16, 8, 8), (16, 16, F16, 4, 8), (4, 4, F16, 8, 6), (4, 4, F16, 4, 6)])
+def test_mrhs_dslash_matches_single(cuda, soa, vec, ft, nrhs, ny):
+    g = Geometry(max(8, 2 * soa), ny, 4, 4, soalen=soa, veclen=vec, ftype=ft, compress12=True, t_boundary=-1.0)
     f = H.make_fields(g, cb=0, seed=61)
     T = lambda a: H.to_torch(a, cuda)
     gauge = T(f["gauge"])
