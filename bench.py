@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bound of the CPU baseline sample")
     ap.add_argument("--no-extras", action="store_true", help="skip the multi-RHS and solver measurements")
-    ap.add_argument("--only", choices=["mrhs", "force", "batch", "solve", "tm"],
+    ap.add_argument("--only", choices=["mrhs", "force", "batch", "solve", "tm", "solve_tm"],
                     help="run one secondary measurement alone (on --dims) and print its JSON line")
     return ap.parse_args()
 
@@ -305,6 +305,76 @@ def bench_solve(dims, dev, nrhs=8, kappa=0.16):
                                    "outer_iters": r16[1]["outer_iters"], "max_rel_res": max(r16[1]["rel_res"])}
     out["speedup_vs_fp32_fp64_single_rhs"] = t32 / t16
     out["speedup_vs_fp64_cg"] = t64 / t16
+    return out
+
+
+def bench_solve_tm(dev, dims=(48, 48, 48, 96), kappa=0.16, mu=0.01):
+    """Even-odd twisted-mass system at 48^3x96, M = 1/(2 kappa) (1 + i mu~
+    gamma5) - D/2 with mu~ = 2 kappa mu (in the operator's convention alpha =
+    1/(2 kappa), mu = mu~ and muinv = alpha / (alpha^2 + mu^2) with the
+    untwisted mu; hopping coefficient 1/2), solved for one Gaussian source to |b - Mhat x|/|b| <=
+    1e-10 by (a) FP64 CG on Mhat^dag Mhat, (b) FP32 CG corrected in FP64,
+    (c) FP16 + per-site norm CG corrected in FP64 (the configuration's
+    storage).  The residual of every solution is recomputed with the FP64
+    operator.  Each path runs once untimed on a loose tolerance, then three
+    times; the median is reported."""
+    from qphix_b200 import fields, layout
+    from qphix_b200.lattice import F16N, F32, F64, Geometry
+    from qphix_b200.solver import EvenOddOperator, mixed_solve
+    G = Geometry(*dims, soalen=8, veclen=8, compress12=True, t_boundary=-1.0, ftype=F64)
+    U = fields.random_gauge(G, seed=177, device=dev)
+    gauge = [layout.pack_gauge(G, U, cb, torch.float64) for cb in (0, 1)]
+    del U
+    alpha = 1.0 / (2 * kappa)
+    p = dict(coeff_s=0.5, coeff_t_f=0.5, coeff_t_b=0.5, alpha=alpha, mu=mu / alpha,
+             muinv=alpha / (alpha ** 2 + mu ** 2))
+    ops_ = {}
+    for ft, dt in ((F64, torch.float64), (F32, torch.float32), (F16N, torch.float16)):
+        ops_[ft] = EvenOddOperator(G.with_(ftype=ft), "tm", gauge=[x.to(dt) for x in gauge], target_cb=1, **p)
+    del gauge
+    b = layout.pack_spinor(G, fields.random_spinor(G, seed=181, device=dev), torch.float64)
+    out = {"lattice": list(dims), "family": "tm", "kappa": kappa, "mu": mu, "tol": 1e-10,
+           "inner_storage": "fp16 + per-site norm (links fp16, 12-real)", "soalen": 8}
+    ops_[F64].cg(b, tol=1e-4, max_iter=50)
+    mixed_solve(ops_[F64], ops_[F32], b, tol=1e-4, inner_tol=1e-2)
+    mixed_solve(ops_[F64], ops_[F16N], b, tol=1e-4, inner_tol=1e-2)
+
+    def timed(fn, reps=3):
+        ts = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return statistics.median(ts), r, ts
+
+    def true_res(x):
+        r = ops_[F64].apply(x)
+        return float((b - r).norm() / b.norm())
+
+    def fp64_cg():
+        """CG on the normal equations stops on |Mhat^dag r| / |Mhat^dag b|;
+        continue from its solution with a tighter bound until the FP64
+        residual |b - Mhat x| / |b| is <= 1e-10"""
+        x, info = ops_[F64].cg(b, tol=1e-10, max_iter=5000)
+        iters, tol = info["iters"], 1e-10
+        while info["rel_res"] > 1e-10 and tol > 1e-13:
+            tol *= 0.5
+            x, info = ops_[F64].cg(b, x=x, tol=tol, max_iter=5000)
+            iters += info["iters"]
+        return x, dict(info, iters=iters)
+
+    t64, r64, a64 = timed(fp64_cg)
+    out["fp64_cg"] = {"seconds": t64, "runs": a64, "iters": r64[1]["iters"], "rel_res": true_res(r64[0])}
+    t32, r32, a32 = timed(lambda: mixed_solve(ops_[F64], ops_[F32], b, tol=1e-10, inner_tol=1e-5))
+    out["fp32_fp64_mixed"] = {"seconds": t32, "runs": a32, "inner_iters": r32[1]["inner_iters"],
+                              "outer_iters": r32[1]["outer_iters"], "rel_res": true_res(r32[0])}
+    t16, r16, a16 = timed(lambda: mixed_solve(ops_[F64], ops_[F16N], b, tol=1e-10, inner_tol=1e-2))
+    out["fp16n_fp64_mixed"] = {"seconds": t16, "runs": a16, "inner_iters": r16[1]["inner_iters"],
+                               "outer_iters": r16[1]["outer_iters"], "rel_res": true_res(r16[0])}
+    out["speedup_vs_fp64_cg"] = t64 / t16
+    out["speedup_vs_fp32_fp64_mixed"] = t32 / t16
     return out
 
 
@@ -622,6 +692,7 @@ def b200_arm(args, world, rank, local):
         extras["force"] = bench_force(dev)
         extras["batch"] = bench_batch(dev, peak)
         extras["tm_fp16n"] = bench_tm(dev)
+        extras["solve_tm"] = bench_solve_tm(dev)
 
     if rank == 0:
         line = {
@@ -662,6 +733,8 @@ def run_only(args):
         r = bench_batch(dev, measured_peak()[0])
     elif args.only == "tm":
         r = bench_tm(dev, dims)
+    elif args.only == "solve_tm":
+        r = bench_solve_tm(dev, dims)
     else:
         r = bench_solve(dims, dev)
     print(json.dumps({"only": args.only, "dims": list(dims), "result": r}))

@@ -54,12 +54,54 @@ template <typename FT, int S, bool COMP12> struct AsyncCfg {
   static constexpr int LKB = R * 6 * S * (int)sizeof(elem_t<FT>);    // link slab bytes
   static constexpr int LKS = St::stride(R * 6);
   static constexpr int HOP = St::G * (St::SP + LKS);                 // one hop's staged bytes
-  static constexpr int BUF = (2 * HOP > St::G * St::CL) ? 2 * HOP : St::G * St::CL;
+  static constexpr int XOFF = (2 * HOP > St::G * St::CL) ? 2 * HOP : St::G * St::CL;
+  // 16-bit storage: an x region, staged once for both x hops, holds blocks
+  // blk0-1 .. blk0+G, the first block of the warp's first row and the last
+  // block of its last row -- every x neighbour of the warp's sites, also
+  // when a row of the lattice does not start or end with the warp.  (For
+  // 32-bit storage it would not fit next to four warps' hop buffers; x
+  // neighbours outside the warp's own blocks are then read from global
+  // memory.)
+  static constexpr bool XREG = sizeof(elem_t<FT>) == 2;
+  static constexpr int XS = St::G + 4;
+  static constexpr int BUF = XOFF + (XREG ? XS * St::SP : 0);
 };
 
 template <typename FT, int S> constexpr bool async_layout()
 {
   return (S == 4 || S == 8 || S == 16) && sizeof(elem_t<FT>) <= 4;
+}
+
+// copy the x region of psi (AsyncCfg::XS blocks) to w.xr; blocks outside
+// the field are skipped (their slots are never read)
+template <typename FT, int S, bool COMP12>
+__device__ __forceinline__ void stage_xregion(const elem_t<FT> *__restrict__ f, long long blk0, long long head,
+                                              long long tail, long long nblocks, unsigned char *xr, int ln)
+{
+  typedef AsyncCfg<FT, S, COMP12> A;
+  typedef Stage<FT, S> St;
+  constexpr int CH = A::SPB / 16, N = CH * A::XS, ROUNDS = (N + 31) / 32;
+  static_assert(A::SPB % 16 == 0, "staged blocks are whole 16-byte vectors");
+  const uint4 *base = reinterpret_cast<const uint4 *>(f);
+#pragma unroll
+  for (int r = 0; r < ROUNDS; r++) {
+    const int j = ln + 32 * r;
+    const int slot = j / CH, c = j - slot * CH;
+    const long long b = slot < St::G + 2 ? blk0 - 1 + slot : (slot == St::G + 2 ? head : tail);
+    if (j < N && b >= 0 && b < nblocks) cp_async16(xr + slot * St::SP + c * 16, base + b * CH + c);
+  }
+}
+
+// x neighbour of site s in direction D (0: back, 1: forward): its block
+// within the row and its lane
+template <int S, int D>
+__device__ __forceinline__ void x_neighbour(const GeoDev &g, const Site &s, int &xb, int &ln)
+{
+  int x = s.xcb;
+  if (D == 0 && s.par == 0) x = x > 0 ? x - 1 : g.nxh - 1;
+  if (D == 1 && s.par == 1) x = x < g.nxh - 1 ? x + 1 : 0;
+  xb = x / S;
+  ln = x % S;
 }
 
 // issue the copies of hop D into buf
@@ -69,9 +111,11 @@ __device__ __forceinline__ void prefetch_hop(const KArgs<FT> &a, const GeoDev &g
 {
   typedef AsyncCfg<FT, S, COMP12> A;
   typedef Stage<FT, S> St;
-  bool cross;
-  const long long nbase = obase + neighbour_offset<S, D>(g, s, (long long)St::SPB * S, 1, &cross);
-  stage_in_async<FT, S, A::SPB, St::SP>(a.psi, D < 2 ? w.own : nbase - w.lane, buf, w.ln);
+  if (!(A::XREG && D < 2)) {
+    bool cross;
+    const long long nbase = obase + neighbour_offset<S, D>(g, s, (long long)St::SPB * S, 1, &cross);
+    stage_in_async<FT, S, A::SPB, St::SP>(a.psi, D < 2 ? w.own : nbase - w.lane, buf, w.ln);
+  }
   stage_in_async<FT, S, A::LKB, A::LKS>(a.gauge, w.tile * (8LL * A::R * 6 * S) + (long long)D * A::R * 6 * S,
                                         buf + St::G * St::SP, w.ln);
 }
@@ -91,7 +135,14 @@ __device__ __forceinline__ void compute_hop(const KArgs<FT> &a, const GeoDev &g,
   const long long nbase = obase + neighbour_offset<S, D>(g, s, (long long)St::SPB * S, 1, &cross);
   if (cross && !((p.acc_mask >> D) & 1u)) return;
   cx<C> psi[4][3], G[3][3];
-  if (MU == 0) {
+  if (MU == 0 && A::XREG) {
+    int xb, nl;
+    x_neighbour<S, D>(g, s, xb, nl);
+    // slot of the row's first block, then of the neighbour's block
+    int sl = (int)(w.blk - w.blk0) + 1 - s.xcb / S + xb;
+    sl = (sl >= 0 && sl < St::G + 2) ? sl : (sl == w.xhead ? St::G + 2 : St::G + 3);
+    load_spinor_sm<FT, S>(w.xr + sl * St::SP, nl, psi);
+  } else if (MU == 0) {
     const long long nb = nbase / (St::SPB * S);
     const int nl = (int)(nbase - nb * (St::SPB * S));
     const long long gi = nb - w.blk0;
@@ -179,6 +230,13 @@ __device__ __forceinline__ void async_body(const KArgs<FT> &a, const GeoDev &g, 
   w.blk = obase / (St::SPB * S);
   w.own = w.blk * (St::SPB * S);
   w.blk0 = __shfl_sync(0xffffffffu, w.blk, 0);
+  if (A::XREG) {
+    // the x region's copies go out now and complete with hop 0's
+    w.xr = buf + A::XOFF;
+    w.xhead = 1 - __shfl_sync(0xffffffffu, s.xcb, 0) / S;
+    const long long tail = __shfl_sync(0xffffffffu, w.blk, 31) - __shfl_sync(0xffffffffu, s.xcb, 31) / S + g.nvecs - 1;
+    stage_xregion<FT, S, COMP12>(a.psi, w.blk0, w.blk0 - 1 + w.xhead, tail, g.Pxyz * g.nt, w.xr, w.ln);
+  }
 
   cx<C> res[4][3];
 #pragma unroll

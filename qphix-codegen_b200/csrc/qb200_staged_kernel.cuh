@@ -216,6 +216,8 @@ struct WarpCtx {
   long long own;     // element index of the site's own spinor block
   long long blk;     // the site's spinor block index
   long long blk0;    // spinor block of the warp's first group
+  unsigned char *xr; // x region (async kernel, 16-bit storage)
+  int xhead;         // x-region slot index of the first row's first block
 };
 
 // y/z/t hop (D = 2..7) or x hop (D = 0, 1) with staged spinor and link
