@@ -235,20 +235,49 @@ template <int S> struct F16NSite {
   }
 };
 
+// The same decode / encode in FP32: the vectors of an FP16 solve carry 11
+// significant bits, so the inner BLAS (axpby, and the per-site terms of the
+// dots, whose sums over sites are FP64) run in FP32 arithmetic.
+template <int S> struct F16NSiteF {
+  static __device__ __forceinline__ void load(const __half *f, long long sl, float (&v)[24])
+  {
+    const long long blk = sl / S;
+    const int l = (int)(sl - blk * S);
+    const __half *b = f + blk * 26 * S;
+    const float nrm = __ldg(reinterpret_cast<const float *>(b + 24 * S) + l);
+#pragma unroll
+    for (int k = 0; k < 24; k++) v[k] = __half2float(b[k * S + l]) * nrm;
+  }
+  static __device__ __forceinline__ void store(__half *f, long long sl, const float (&v)[24])
+  {
+    const long long blk = sl / S;
+    const int l = (int)(sl - blk * S);
+    __half *b = f + blk * 26 * S;
+    float m = 0.f;
+#pragma unroll
+    for (int k = 0; k < 24; k++) m = fmaxf(m, fabsf(v[k]));
+    const float nrm = m > 0.f ? m : 1.0f;
+    reinterpret_cast<float *>(b + 24 * S)[l] = nrm;
+    const float inv = 1.0f / nrm;
+#pragma unroll
+    for (int k = 0; k < 24; k++) b[k * S + l] = __float2half_rn(v[k] * inv);
+  }
+};
+
 // y = a x + b y
 template <int S>
 __global__ void __launch_bounds__(256) axpby_f16n_kernel(long long nsl, ScalarRef a, const __half *__restrict__ x,
                                                          ScalarRef b, __half *__restrict__ y)
 {
-  const double av = a.get(), bv = b.get();
+  const float av = (float)a.get(), bv = (float)b.get();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nsl;
        i += (long long)gridDim.x * blockDim.x) {
-    double vx[24], vy[24];
-    F16NSite<S>::load(x, i, vx);
-    F16NSite<S>::load(y, i, vy);
+    float vx[24], vy[24];
+    F16NSiteF<S>::load(x, i, vx);
+    F16NSiteF<S>::load(y, i, vy);
 #pragma unroll
     for (int k = 0; k < 24; k++) vy[k] = av * vx[k] + bv * vy[k];
-    F16NSite<S>::store(y, i, vy);
+    F16NSiteF<S>::store(y, i, vy);
   }
 }
 
@@ -258,22 +287,24 @@ __global__ void __launch_bounds__(256) caxpby_f16n_kernel(long long nsl, double 
                                                           const __half *__restrict__ x, double br, double bi,
                                                           __half *__restrict__ y)
 {
+  const float fr = (float)ar, fi = (float)ai, gr = (float)br, gi = (float)bi;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nsl;
        i += (long long)gridDim.x * blockDim.x) {
-    double vx[24], vy[24];
-    F16NSite<S>::load(x, i, vx);
-    F16NSite<S>::load(y, i, vy);
+    float vx[24], vy[24];
+    F16NSiteF<S>::load(x, i, vx);
+    F16NSiteF<S>::load(y, i, vy);
 #pragma unroll
     for (int j = 0; j < 12; j++) {
-      const double xr = vx[2 * j], xi = vx[2 * j + 1], yr = vy[2 * j], yi = vy[2 * j + 1];
-      vy[2 * j] = ar * xr - ai * xi + br * yr - bi * yi;
-      vy[2 * j + 1] = ar * xi + ai * xr + br * yi + bi * yr;
+      const float xr = vx[2 * j], xi = vx[2 * j + 1], yr = vy[2 * j], yi = vy[2 * j + 1];
+      vy[2 * j] = fr * xr - fi * xi + gr * yr - gi * yi;
+      vy[2 * j + 1] = fr * xi + fi * xr + gr * yi + gi * yr;
     }
-    F16NSite<S>::store(y, i, vy);
+    F16NSiteF<S>::store(y, i, vy);
   }
 }
 
-// partials: real dot (CPLX = false) or complex <x, y> (CPLX = true)
+// partials: real dot (CPLX = false) or complex <x, y> (CPLX = true); each
+// site's 24 terms are summed in FP32, the sites in FP64
 template <int S, bool CPLX>
 __global__ void __launch_bounds__(kRedThreads) dot_f16n_partial_kernel(long long nsl, const __half *__restrict__ x,
                                                                        const __half *__restrict__ y,
@@ -282,19 +313,22 @@ __global__ void __launch_bounds__(kRedThreads) dot_f16n_partial_kernel(long long
   double re = 0.0, im = 0.0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nsl;
        i += (long long)gridDim.x * blockDim.x) {
-    double vx[24], vy[24];
-    F16NSite<S>::load(x, i, vx);
-    F16NSite<S>::load(y, i, vy);
+    float vx[24], vy[24];
+    F16NSiteF<S>::load(x, i, vx);
+    F16NSiteF<S>::load(y, i, vy);
+    float sr = 0.f, si = 0.f;
     if (CPLX) {
 #pragma unroll
       for (int j = 0; j < 12; j++) {
-        re += vx[2 * j] * vy[2 * j] + vx[2 * j + 1] * vy[2 * j + 1];
-        im += vx[2 * j] * vy[2 * j + 1] - vx[2 * j + 1] * vy[2 * j];
+        sr += vx[2 * j] * vy[2 * j] + vx[2 * j + 1] * vy[2 * j + 1];
+        si += vx[2 * j] * vy[2 * j + 1] - vx[2 * j + 1] * vy[2 * j];
       }
     } else {
 #pragma unroll
-      for (int k = 0; k < 24; k++) re += vx[k] * vy[k];
+      for (int k = 0; k < 24; k++) sr += vx[k] * vy[k];
     }
+    re += (double)sr;
+    im += (double)si;
   }
   block_sum2(re, im);
   if (threadIdx.x == 0) {
