@@ -2,7 +2,9 @@
 TSlabDslash (face pack -> exchange -> body without the slab-crossing hops ->
 face unpack) with the oracle as the compute kernels, and must reproduce the
 oracle applied to the whole lattice, for every family, kernel and sign, with
-twisted boundary phases in t and an antiperiodic time boundary."""
+twisted boundary phases in t and an antiperiodic time boundary.  The slab
+CG (TSlabEvenOdd + cg, inner products all-reduced) must solve the whole
+lattice's even-odd system to 1e-10 for every family."""
 import os
 import socket
 
@@ -15,7 +17,7 @@ import torch.multiprocessing as mp
 import helpers as H
 import oracle as O
 from qphix_b200 import fields, layout
-from qphix_b200.halo import TComm, TSlabDslash, local_geometry
+from qphix_b200.halo import TComm, TSlabDslash, TSlabEvenOdd, cg, local_geometry
 from qphix_b200.lattice import F64, Geometry
 
 
@@ -41,6 +43,12 @@ class OracleKernels:
         cl = kw.pop("clover")
         O.face_unpack(g, family, isign, cb, buf.numpy(), gauge.numpy(), out.numpy(), dir,
                       clover=cl.numpy() if cl is not None else None, **kw)
+
+    def axpby(self, a, x, b, y):
+        y.mul_(b).add_(x, alpha=a)
+
+    def dot(self, x, y):
+        return float(torch.dot(x, y))
 
 
 def _fields(G, cb):
@@ -117,3 +125,72 @@ def test_two_rank_t_slabs_match_global_oracle():
                     exp = ref_c[rank * g.nt:(rank + 1) * g.nt]
                     err = float((got - exp).abs().max())
                     assert err < 1e-12, (fam, kernel, isign, rank, err)
+
+
+EO_G = dict(nx=4, ny=4, nz=4, nt=8, soalen=2, veclen=4, ftype=F64, compress12=True, t_boundary=-1.0)
+
+
+def _eo_canonical(G, family, seed=900, target_cb=1):
+    """The canonical fields behind helpers.eo_setup (same seeds): links,
+    per-checkerboard clover terms (A on the target, A^-1 on the other) and
+    their adjoints, and the source on the target checkerboard."""
+    other = 1 - target_cb
+    c = {"U": fields.random_gauge(G, seed=seed), "clov": [None, None], "clov_dag": [None, None],
+         "b": fields.random_spinor(G, seed=seed + 3)}
+    if family == "clover":
+        c["clov"][target_cb] = fields.random_clover(G, seed=seed + 1)
+        c["clov"][other] = fields.invert_blocks(fields.random_clover(G, seed=seed + 2))
+    if family == "tm_clover":
+        c["clov"][target_cb] = fields.random_full_clover(G, seed=seed + 1)
+        c["clov"][other] = fields.invert_blocks(fields.random_full_clover(G, seed=seed + 2))
+        c["clov_dag"] = [m.conj().transpose(-1, -2) for m in c["clov"]]
+    return c
+
+
+def _cg_worker(rank, world, port, results):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        G = Geometry(**EO_G)
+        g = local_geometry(G, rank, world)
+        t0, nt = rank * g.nt, g.nt
+        sl = slice(t0, t0 + nt)
+        out = {}
+        for fam in H.FAMILIES:
+            _, p = H.eo_setup(G, fam)
+            c = _eo_canonical(G, fam)
+            pack = layout.pack_full_clover if fam == "tm_clover" else layout.pack_clover
+            cl = [pack(g, m[sl]) if m is not None else None for m in c["clov"]]
+            cld = [pack(g, m[sl]) if m is not None else None for m in c["clov_dag"]]
+            gauge = [layout.pack_gauge(g, c["U"], cb, t0=t0) for cb in (0, 1)]
+            op = TSlabEvenOdd(TSlabDslash(g, TComm(), OracleKernels()), fam, gauge, clov=cl, clov_dag=cld,
+                              target_cb=1, **p)
+            x, info = cg(op, layout.pack_spinor(g, c["b"][sl]), tol=1e-11, max_iter=500)
+            out[fam] = (x.numpy(), info)
+        results[rank] = out
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_slab_cg_solves_global_system():
+    world = 2
+    mgr = mp.Manager()
+    results = mgr.dict()
+    mp.start_processes(_cg_worker, args=(world, _free_port(), results), nprocs=world, start_method="spawn")
+    G = Geometry(**EO_G)
+    for fam in H.FAMILIES:
+        f, p = H.eo_setup(G, fam)
+        parts, infos = [], []
+        for rank in range(world):
+            x, info = results[rank][fam]
+            parts.append(layout.unpack_spinor(local_geometry(G, rank, world), torch.from_numpy(x)))
+            infos.append(info)
+        # the ranks leave the loop together with the same global residual
+        assert infos[0]["iters"] == infos[1]["iters"] > 0, (fam, infos)
+        assert abs(infos[0]["rel_res"] - infos[1]["rel_res"]) <= 1e-15, (fam, infos)
+        x = layout.pack_spinor(G, torch.cat(parts)).numpy()
+        mx = H.oracle_schur(G, fam, f, p, x)
+        rel = float(np.linalg.norm(f["b"] - mx) / np.linalg.norm(f["b"]))
+        assert rel <= 1e-10, (fam, rel, infos[0])
+        assert abs(rel - infos[0]["rel_res"]) <= 1e-12, (fam, rel, infos[0])

@@ -109,3 +109,23 @@ def test_mixed_precision_reaches_1e10(cuda, lo, solver):
     assert info["rel_res"] <= 1e-10, info
     assert _true_res(g, family, f, p, x.cpu().numpy()) < 2e-10
     print(solver, lo, info)
+
+
+@pytest.mark.parametrize("family", ["clover", "tm_clover"])
+def test_slab_cg_single_rank(cuda, family):
+    """halo.cg over TSlabEvenOdd with the GPU kernels and the library's FP64
+    BLAS (one rank: no exchange) solves the even-odd system to 1e-10."""
+    from qphix_b200.halo import GPUKernels, TComm, TSlabDslash, TSlabEvenOdd, cg
+    g = Geometry(8, 8, 8, 8, soalen=4, veclen=8, ftype=F64, compress12=True, t_boundary=-1.0)
+    f, p = H.eo_setup(g, family)
+    T = lambda a: None if a is None else torch.from_numpy(np.ascontiguousarray(a)).to(cuda)
+    op = TSlabEvenOdd(TSlabDslash(g, TComm(), GPUKernels(torch.float64, cuda)), family,
+                      [T(x) for x in f["gauge"]], clov=[T(x) for x in f["clov"]],
+                      clov_dag=[T(x) for x in f["clov_dag"]], target_cb=1, **p)
+    b = T(f["b"])
+    x, info = cg(op, b, tol=1e-11, max_iter=2000)
+    assert info["rel_res"] <= 1e-10, info
+    assert _true_res(g, family, f, p, x.cpu().numpy()) < 1e-10
+    # same iterate count as the library's CG on the same system
+    x2, info2 = _op(g, family, f, p, cuda).cg(b, tol=1e-11, max_iter=2000)
+    assert abs(info["iters"] - info2["iters"]) <= 2, (info, info2)
