@@ -409,6 +409,11 @@ int qb200_invert_bicgstab(const qb200_lattice *lat, const qb200_operator *op, co
  * high-precision lattice (FP64 storage), corrections solved with the
  * low-precision lattice (FP32 or FP16 storage; its operator fields in that
  * type) to inner_tol.  solver 0: CG on the normal equations, 1: BiCGStab.
+ * solver 2: one CG on the normal equations in the low precision with FP64
+ * reliable updates (no restarts): x accumulates in FP64 and the FP64
+ * residual replaces the low-precision one whenever the latter has fallen by
+ * the factor inner_tol (0 < inner_tol < 1); max_inner bounds the
+ * iterations, max_outer the updates.
  * Returns the high workspace size; *lo_bytes receives the low one. */
 long long qb200_mixed_workspace_bytes(const qb200_lattice *lat_hi, const qb200_lattice *lat_lo,
                                       long long *lo_bytes);

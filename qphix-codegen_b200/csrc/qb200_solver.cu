@@ -775,11 +775,104 @@ int qb200_invert_bicgstab(const qb200_lattice *lat, const qb200_operator *op, co
   return QB200_OK;
 }
 
+// CG on the normal equations in the low precision with reliable updates:
+// one Krylov space for the whole solve (no restarts).  Each segment starts
+// from the FP64 residual r = b - Mhat x, its normal form rn = Mhat^dag r,
+// scaled to O(1) components and demoted; the low-precision CG then iterates
+// r_lo, p_lo and a low-precision increment x_lo.  When |r_lo| has fallen by
+// the factor delta since the segment started (or far enough that the
+// segment's FP64 residual, scaled by that fall, would meet rel_tol), x_lo is
+// promoted and added to x in FP64, the FP64 residual is recomputed and
+// replaces r_lo, and p_lo is rescaled to the new segment's units, so the
+// search direction survives the update.
+static int reliable_cg(const qb200_lattice *lat_hi, const qb200_operator *op_hi, const qb200_lattice *lat_lo,
+                       const qb200_operator *op_lo, const void *b, void *x, double rel_tol, double delta,
+                       int max_iter, int max_updates, const Vecs &H, const Vecs &L, int *iters, int *updates,
+                       double *rel_out, cudaStream_t st)
+{
+  const VS VH = vs_of(lat_hi), VL = vs_of(lat_lo);
+  const double ncomp = (double)VH.n;
+  void *r = H.v[0], *rn = H.v[1], *e_hi = H.v[2], *tmp = H.v[3];
+  void *rl = L.v[0], *p = L.v[1], *Ap = L.v[2], *t = L.v[3], *tl = L.v[4], *xl = L.v[8];
+  double *d = L.scal;
+  int rc;
+  cudaError_t e;
+  double rel = 1.0;
+  if ((rc = true_residual(lat_hi, op_hi, b, x, r, tmp, H.partials, H.scal + 2, &rel, st))) return rc;
+  int k = 0, nup = 0;
+  double scale = 1.0, rr = 0.0, seg_rr = 0.0, seg_rel = rel;
+  bool first = true;
+  while (rel > rel_tol && k < max_iter) {
+    // new segment from the FP64 residual r (x_lo = 0)
+    if ((rc = schur(lat_hi, op_hi, 0, r, rn, tmp, st))) return rc;
+    double rrh;
+    e = dot(VH, rn, rn, H.partials, H.scal + 4, st);
+    if ((rc = cuda_rc(e, "reliable cg norm"))) return rc;
+    if ((rc = fetch(&rrh, H.scal + 4, 1, st))) return rc;
+    const double s_new = std::sqrt(ncomp / (rrh > 0 ? rrh : 1.0));
+    e = convert(VL, rl, VH, rn, s_new, st);
+    if (e == cudaSuccess) e = first ? cudaMemcpyAsync(p, rl, spinor_bytes(lat_lo), cudaMemcpyDeviceToDevice, st)
+                                    : axpby(VL, host(0.0), rl, host(s_new / scale), p, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(xl, 0, spinor_bytes(lat_lo), st);
+    if (e == cudaSuccess) e = dot(VL, rl, rl, L.partials, d + 0, st);
+    if ((rc = cuda_rc(e, "reliable cg segment"))) return rc;
+    double rrs;
+    if ((rc = fetch(&rrs, d + 0, 1, st))) return rc;
+    if (!first) {
+      // continue the recurrence in the new units: p = r + beta p
+      const double beta = rrs / (rr * (s_new / scale) * (s_new / scale));
+      e = axpby(VL, host(1.0), rl, host(beta), p, st);
+      if ((rc = cuda_rc(e, "reliable cg direction"))) return rc;
+    }
+    scale = s_new;
+    rr = seg_rr = rrs;
+    seg_rel = rel;
+    first = false;
+    bool update = false;
+    while (!update && k < max_iter) {
+      if ((rc = normal_op(lat_lo, op_lo, p, Ap, t, tl, st))) return rc;
+      e = dot(VL, p, Ap, L.partials, d + 1, st);
+      if ((rc = cuda_rc(e, "reliable cg pAp"))) return rc;
+      double pAp;
+      if ((rc = fetch(&pAp, d + 1, 1, st))) return rc;
+      const double alpha = rr / pAp;
+      e = axpby(VL, host(alpha), p, host(1.0), xl, st);
+      if (e == cudaSuccess) e = axpby(VL, host(-alpha), Ap, host(1.0), rl, st);
+      if (e == cudaSuccess) e = dot(VL, rl, rl, L.partials, d + 2, st);
+      if ((rc = cuda_rc(e, "reliable cg iteration"))) return rc;
+      double rrn;
+      if ((rc = fetch(&rrn, d + 2, 1, st))) return rc;
+      k++;
+      if (!std::isfinite(rrn) || !std::isfinite(alpha)) return api_fail(QB200_EINVAL, "cg: residual is not finite");
+      update = rrn <= delta * delta * seg_rr || seg_rel * std::sqrt(rrn / seg_rr) <= rel_tol || k == max_iter;
+      if (!update) {
+        e = axpby(VL, host(1.0), rl, host(rrn / rr), p, st);
+        if ((rc = cuda_rc(e, "reliable cg direction"))) return rc;
+        rr = rrn;
+      }
+      // on an update rr keeps |r|^2 of the step before: the next direction's
+      // beta divides the replaced residual's |r|^2 by it
+    }
+    // x += x_lo / scale in FP64, then the FP64 residual
+    e = convert(VH, e_hi, VL, xl, 1.0 / scale, st);
+    if (e == cudaSuccess) e = axpby(VH, host(1.0), e_hi, host(1.0), x, st);
+    if ((rc = cuda_rc(e, "reliable cg update"))) return rc;
+    if ((rc = true_residual(lat_hi, op_hi, b, x, r, tmp, H.partials, H.scal + 2, &rel, st))) return rc;
+    if (++nup >= max_updates) break;
+  }
+  *iters = k;
+  *updates = nup;
+  *rel_out = rel;
+  return QB200_OK;
+}
+
 // Defect correction: the true residual r = b - Mhat x is formed in the high
 // precision (FP64 storage), the correction solved in the low precision
 // (FP32 or FP16 storage, FP32 arithmetic) to inner_tol, and accumulated in
 // high precision, until |r|/|b| <= rel_tol.  solver: 0 CG on the normal
-// equations, 1 BiCGStab.
+// equations, 1 BiCGStab.  solver 2: CG on the normal equations with reliable
+// updates (reliable_cg; inner_tol is the fall of the low-precision residual
+// between FP64 updates, max_inner the iterations, max_outer the updates).
 int qb200_invert_mixed(const qb200_lattice *lat_hi, const qb200_operator *op_hi, const qb200_lattice *lat_lo,
                        const qb200_operator *op_lo, int solver, const void *b, void *x, double rel_tol,
                        double inner_tol, int max_inner, int max_outer, void *ws_hi, void *ws_lo,
@@ -790,7 +883,10 @@ int qb200_invert_mixed(const qb200_lattice *lat_hi, const qb200_operator *op_hi,
   if ((rc = check_op(lat_lo, op_lo))) return rc;
   if (!same_shape(lat_hi, lat_lo)) return api_fail(QB200_EINVAL, "high and low precision lattices differ in shape");
   if (!b || !x || !ws_hi || !ws_lo) return api_fail(QB200_ENULL, "b, x and workspaces must be non-NULL");
-  if (solver != 0 && solver != 1) return api_fail(QB200_EINVAL, "solver must be 0 (CG) or 1 (BiCGStab)");
+  if (solver < 0 || solver > 2)
+    return api_fail(QB200_EINVAL, "solver must be 0 (CG), 1 (BiCGStab) or 2 (CG with reliable updates)");
+  if (solver == 2 && !(inner_tol > 0.0 && inner_tol < 1.0))
+    return api_fail(QB200_EINVAL, "reliable updates need 0 < inner_tol < 1");
   cudaStream_t st = (cudaStream_t)stream;
   const VS VH = vs_of(lat_hi), VL = vs_of(lat_lo);
   const double ncomp = (double)VH.n; // components of one high-precision spinor array
@@ -808,6 +904,15 @@ int qb200_invert_mixed(const qb200_lattice *lat_hi, const qb200_operator *op_hi,
   }
   int tot = 0, outer = 0;
   double rel = 1.0;
+  if (solver == 2) {
+    if ((rc = reliable_cg(lat_hi, op_hi, lat_lo, op_lo, b, x, rel_tol, inner_tol, max_inner, max_outer, H, L, &tot,
+                          &outer, &rel, st)))
+      return rc;
+    if (inner_iters) *inner_iters = tot;
+    if (outer_iters) *outer_iters = outer;
+    if (rel_res) *rel_res = rel;
+    return QB200_OK;
+  }
   while (outer < max_outer) {
     // r = b - Mhat x (high precision)
     if ((rc = true_residual(lat_hi, op_hi, b, x, r, tmp, H.partials, H.scal + 2, &rel, st))) return rc;

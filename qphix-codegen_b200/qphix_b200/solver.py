@@ -98,12 +98,23 @@ class EvenOddOperator:
         return self._solve("qb200_invert_bicgstab", "qb200_bicgstab_workspace_bytes", b, x, tol, max_iter)
 
 
+SOLVERS = {"cg": 0, "bicgstab": 1, "cg_reliable": 2}
+
+
 def mixed_solve(op_hi: EvenOddOperator, op_lo: EvenOddOperator, b, solver="cg", tol=1e-10, inner_tol=1e-3,
                 max_inner=10000, max_outer=50, x=None):
-    """Defect-correction solve: FP64 residual and solution (op_hi must use
-    FP64 storage), corrections from op_lo (FP32 or FP16 storage)."""
+    """Mixed-precision solve with the FP64 residual and solution in op_hi
+    (FP64 storage) and the iterations in op_lo (FP32, FP16, FP16 + norm or
+    BF16 storage).  solver "cg" / "bicgstab": defect correction, each
+    correction solved to inner_tol (max_inner iterations, max_outer
+    corrections).  solver "cg_reliable": one CG on the normal equations with
+    reliable updates -- the FP64 residual replaces the low-precision one
+    whenever the latter has fallen by inner_tol, keeping the search direction
+    (max_inner iterations in all, max_outer updates)."""
     if op_hi.g.ftype != F64:
         raise ValueError("the high-precision operator must use FP64 storage")
+    if solver not in SOLVERS:
+        raise ValueError("unknown solver %r" % solver)
     L = _lib.lib()
     lo = ctypes.c_longlong(0)
     hi = L.qb200_mixed_workspace_bytes(ctypes.byref(op_hi.lat), ctypes.byref(op_lo.lat), ctypes.byref(lo))
@@ -111,7 +122,7 @@ def mixed_solve(op_hi: EvenOddOperator, op_lo: EvenOddOperator, b, solver="cg", 
     x = x if x is not None else op_hi._spinor()
     ii, oo, rel = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_double(0.0)
     _lib.check(L.qb200_invert_mixed(ctypes.byref(op_hi.lat), ctypes.byref(op_hi.op), ctypes.byref(op_lo.lat),
-                                    ctypes.byref(op_lo.op), 0 if solver == "cg" else 1, _ptr(b), _ptr(x), tol,
+                                    ctypes.byref(op_lo.op), SOLVERS[solver], _ptr(b), _ptr(x), tol,
                                     inner_tol, max_inner, max_outer, _ptr(ws_hi), _ptr(ws_lo), ctypes.byref(ii),
                                     ctypes.byref(oo), ctypes.byref(rel), _stream()))
     return x, {"inner_iters": ii.value, "outer_iters": oo.value, "rel_res": rel.value}

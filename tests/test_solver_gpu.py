@@ -96,7 +96,7 @@ def test_cg_and_bicgstab_fp64(cuda, family):
 
 
 @pytest.mark.parametrize("lo", [F32, F16, F16N, BF16])
-@pytest.mark.parametrize("solver", ["cg", "bicgstab"])
+@pytest.mark.parametrize("solver", ["cg", "bicgstab", "cg_reliable"])
 def test_mixed_precision_reaches_1e10(cuda, lo, solver):
     family = "clover"
     g = Geometry(8, 8, 8, 8, soalen=4, veclen=8, ftype=F64, compress12=True, t_boundary=-1.0)
@@ -105,7 +105,8 @@ def test_mixed_precision_reaches_1e10(cuda, lo, solver):
     glo = g.with_(ftype=lo)
     oplo = _op(glo, family, f, p, cuda, dtype=glo.dtype)   # links / clover in the low type
     b = torch.from_numpy(f["b"]).to(cuda)
-    x, info = mixed_solve(op64, oplo, b, solver=solver, tol=1e-10, inner_tol=1e-4 if lo == F32 else 1e-2)
+    inner = (1e-4 if lo == F32 else 1e-2) if solver != "cg_reliable" else (1e-3 if lo == F32 else 0.1)
+    x, info = mixed_solve(op64, oplo, b, solver=solver, tol=1e-10, inner_tol=inner)
     assert info["rel_res"] <= 1e-10, info
     assert _true_res(g, family, f, p, x.cpu().numpy()) < 2e-10
     print(solver, lo, info)
@@ -129,3 +130,32 @@ def test_slab_cg_single_rank(cuda, family):
     # same iterate count as the library's CG on the same system
     x2, info2 = _op(g, family, f, p, cuda).cg(b, tol=1e-11, max_iter=2000)
     assert abs(info["iters"] - info2["iters"]) <= 2, (info, info2)
+
+
+@pytest.mark.parametrize("family", ["wilson", "tm", "tm_clover"])
+def test_reliable_updates_fp16n(cuda, family):
+    """CG with FP64 reliable updates on FP16 + norm storage for the other
+    families: 1e-10 against the oracle, and no more iterations than defect
+    correction needs."""
+    g = Geometry(16, 8, 8, 8, soalen=8, veclen=8, ftype=F64, compress12=True, t_boundary=-1.0)
+    f, p = H.eo_setup(g, family)
+    op64 = _op(g, family, f, p, cuda)
+    glo = g.with_(ftype=F16N)
+    oplo = _op(glo, family, f, p, cuda, dtype=glo.dtype)
+    b = torch.from_numpy(f["b"]).to(cuda)
+    x, info = mixed_solve(op64, oplo, b, solver="cg_reliable", tol=1e-10, inner_tol=0.1)
+    assert info["rel_res"] <= 1e-10, info
+    assert _true_res(g, family, f, p, x.cpu().numpy()) < 2e-10
+    _, dc = mixed_solve(op64, oplo, b, solver="cg", tol=1e-10, inner_tol=1e-2)
+    assert info["inner_iters"] <= dc["inner_iters"] + 5, (info, dc)
+
+
+def test_mixed_solver_arguments(cuda):
+    g = Geometry(8, 8, 8, 8, soalen=4, veclen=8, ftype=F64, compress12=True, t_boundary=-1.0)
+    f, p = H.eo_setup(g, "wilson")
+    op64 = _op(g, "wilson", f, p, cuda)
+    b = torch.from_numpy(f["b"]).to(cuda)
+    with pytest.raises(ValueError):
+        mixed_solve(op64, op64, b, solver="gmres")
+    with pytest.raises(RuntimeError):
+        mixed_solve(op64, op64, b, solver="cg_reliable", inner_tol=1.5)
