@@ -466,6 +466,18 @@ int qb200_invert_mixed_mrhs(const qb200_lattice *lat_hi, const qb200_operator *o
                             const qb200_operator *op_lo, int nrhs, const void *const *b, void *const *x,
                             double rel_tol, double inner_tol, int max_inner, int max_outer, void *ws_hi, void *ws_lo,
                             int *inner_iters, int *outer_iters, double *rel_res, void *stream);
+/* Multi-RHS CG on the normal equations in the low precision with FP64
+ * reliable updates, all right-hand sides updated together: x_i accumulate in
+ * FP64, and the residuals b_i - Mhat x_i (FP64) replace the iterated ones
+ * whenever every unconverged right-hand side's iterated residual has fallen
+ * by delta (0 < delta < 1); the recurrence continues (no restart).  Same
+ * arguments and workspaces as qb200_invert_mixed_mrhs; *iters: iterations,
+ * *updates: FP64 updates. */
+int qb200_invert_reliable_mrhs(const qb200_lattice *lat_hi, const qb200_operator *op_hi,
+                               const qb200_lattice *lat_lo, const qb200_operator *op_lo, int nrhs,
+                               const void *const *b, void *const *x, double rel_tol, double delta, int max_iter,
+                               int max_updates, void *ws_hi, void *ws_lo, int *iters, int *updates, double *rel_res,
+                               void *stream);
 
 /* ---- layout converters -------------------------------------------------
  * No counterpart in the reference (QPhiX converts on the host).  Canonical

@@ -542,6 +542,103 @@ int mr_cg_core(const qb200_lattice *l, int nrhs, const qb200_operator *op, const
   return QB200_OK;
 }
 
+// Multi-RHS CG on the normal equations in the low precision with FP64
+// reliable updates, all right-hand sides updated together: each segment
+// starts from the FP64 residuals r_i = b_i - Mhat x_i, scaled to unit rms and
+// packed, their normal form Mhat^dag r (low precision, all right-hand sides
+// in one application) replaces the iterated residual, and p is rescaled to
+// the new units, so the recurrence continues (no restart).  A segment ends
+// when every unconverged right-hand side's iterated residual has fallen by
+// delta, or far enough that its FP64 residual would meet rel_tol; then
+// x_i += x_lo_i / scale_i in FP64.
+int mr_reliable(const qb200_lattice *lat_hi, const qb200_operator *op_hi, const qb200_lattice *lat_lo,
+                const qb200_operator *op_lo, int nrhs, const void *const *b, void *const *x, double rel_tol,
+                double delta, int max_iter, int max_updates, void *r, void *tmp, double *partials, double *scal,
+                MRVecs &L, const double *bnorm, int *iters, int *updates, double *rel, cudaStream_t st)
+{
+  MR m;
+  m.ft = lat_lo->ftype;
+  m.nrhs = nrhs;
+  m.n = qb200_spinor_elems(lat_lo) * nrhs;
+  const long long n1 = qb200_spinor_elems(lat_hi);
+  const size_t bytes = single_bytes(lat_lo) * nrhs;
+  void *rl = L.v[0], *p = L.v[1], *Ap = L.v[2], *t = L.v[3], *tl = L.v[4], *r_lo = L.v[5], *xl = L.v[7];
+  double *rr_d = L.slot(0), *rrn_d = L.slot(1), *pAp_d = L.slot(2);
+  double scale[kMaxRhs], rr[kMaxRhs], seg_rr[kMaxRhs], seg_rel[kMaxRhs], s_new[kMaxRhs], h[kMaxRhs];
+  int k = 0, nup = 0, rc;
+  bool first = true;
+  cudaError_t e;
+  while (true) {
+    bool all = true;
+    for (int i = 0; i < nrhs; i++) {
+      if ((rc = qb200_schur_apply(lat_hi, op_hi, 1, x[i], r, tmp, st))) return rc;
+      if ((rc = qb200_blas_axpby(QB200_F64, n1, 1.0, b[i], -1.0, r, st))) return rc;
+      double rrh;
+      if ((rc = qb200_blas_dot(QB200_F64, n1, r, r, scal, partials, st))) return rc;
+      if ((rc = fetch(&rrh, scal, 1, st))) return rc;
+      rel[i] = bnorm[i] > 0 ? std::sqrt(rrh / bnorm[i]) : 0.0;
+      if (rel[i] > rel_tol) all = false;
+      s_new[i] = std::sqrt((double)n1 / (rrh > 0 ? rrh : 1.0));
+      if ((rc = cuda_rc(mr_slot(true, m.ft, n1, nrhs, i, r, s_new[i], r_lo, st), "multi-RHS pack slot"))) return rc;
+    }
+    if (all || k >= max_iter || nup >= max_updates) break;
+    if ((rc = mr_schur(lat_lo, nrhs, op_lo, 0, r_lo, rl, tl, st))) return rc;
+    VecScalar ratio = vhost(0.0);
+    for (int i = 0; i < nrhs; i++) ratio.host[i] = first ? 1.0 : s_new[i] / scale[i];
+    e = first ? cudaMemcpyAsync(p, rl, bytes, cudaMemcpyDeviceToDevice, st)
+              : mr_axpby(m, vhost(0.0), rl, ratio, p, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(xl, 0, bytes, st);
+    if (e == cudaSuccess) e = mr_dot(m, rl, rl, L.partials, rr_d, st);
+    if ((rc = cuda_rc(e, "multi-RHS reliable segment"))) return rc;
+    if ((rc = fetch(h, rr_d, nrhs, st))) return rc;
+    if (!first) {
+      // continue the recurrence in the new units: p = r + beta p
+      VecScalar beta = vhost(0.0);
+      for (int i = 0; i < nrhs; i++) beta.host[i] = h[i] / (rr[i] * ratio.host[i] * ratio.host[i]);
+      if ((rc = cuda_rc(mr_axpby(m, vhost(1.0), rl, beta, p, st), "multi-RHS reliable direction"))) return rc;
+    }
+    for (int i = 0; i < nrhs; i++) {
+      scale[i] = s_new[i];
+      rr[i] = seg_rr[i] = h[i];
+      seg_rel[i] = rel[i];
+    }
+    first = false;
+    bool update = false;
+    while (!update && k < max_iter) {
+      if ((rc = mr_schur(lat_lo, nrhs, op_lo, 1, p, t, tl, st))) return rc;
+      if ((rc = mr_schur(lat_lo, nrhs, op_lo, 0, t, Ap, tl, st))) return rc;
+      e = mr_dot(m, p, Ap, L.partials, pAp_d, st);
+      if (e == cudaSuccess) e = mr_axpby(m, vratio(rr_d, pAp_d, 1.0), p, vhost(1.0), xl, st);
+      if (e == cudaSuccess) e = mr_axpby(m, vratio(rr_d, pAp_d, -1.0), Ap, vhost(1.0), rl, st);
+      if (e == cudaSuccess) e = mr_dot(m, rl, rl, L.partials, rrn_d, st);
+      if ((rc = cuda_rc(e, "multi-RHS reliable iteration"))) return rc;
+      if ((rc = fetch(h, rrn_d, nrhs, st))) return rc;
+      k++;
+      update = true;
+      for (int i = 0; i < nrhs; i++) {
+        if (!std::isfinite(h[i])) return api_fail(QB200_EINVAL, "multi-RHS cg: residual is not finite");
+        const bool fell = h[i] <= delta * delta * seg_rr[i] || seg_rel[i] * std::sqrt(h[i] / seg_rr[i]) <= rel_tol;
+        if (seg_rel[i] > rel_tol && !fell) update = false;
+      }
+      if (k == max_iter) update = true;
+      if (!update) {
+        e = mr_axpby(m, vhost(1.0), rl, vratio(rrn_d, rr_d, 1.0), p, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(rr_d, rrn_d, nrhs * sizeof(double), cudaMemcpyDeviceToDevice, st);
+        if ((rc = cuda_rc(e, "multi-RHS reliable direction"))) return rc;
+        for (int i = 0; i < nrhs; i++) rr[i] = h[i];
+      }
+      // on an update rr keeps |r|^2 of the step before, for the next beta
+    }
+    for (int i = 0; i < nrhs; i++)
+      if ((rc = cuda_rc(mr_slot_add(m.ft, n1, nrhs, i, xl, 1.0 / scale[i], x[i], st), "multi-RHS update")))
+        return rc;
+    nup++;
+  }
+  *iters = k;
+  *updates = nup;
+  return QB200_OK;
+}
+
 } // namespace
 
 extern "C" {
@@ -637,10 +734,10 @@ long long qb200_mixed_mrhs_workspace_bytes(const qb200_lattice *lat_hi, const qb
 // or FP32 storage) to inner_tol, and the corrections are accumulated into x
 // in FP64.  b and x: host arrays of nrhs device
 // pointers to FP64 single-layout spinors.
-int qb200_invert_mixed_mrhs(const qb200_lattice *lat_hi, const qb200_operator *op_hi, const qb200_lattice *lat_lo,
-                            const qb200_operator *op_lo, int nrhs, const void *const *b, void *const *x,
-                            double rel_tol, double inner_tol, int max_inner, int max_outer, void *ws_hi, void *ws_lo,
-                            int *inner_iters, int *outer_iters, double *rel_res, void *stream)
+static int mixed_mrhs(const qb200_lattice *lat_hi, const qb200_operator *op_hi, const qb200_lattice *lat_lo,
+                      const qb200_operator *op_lo, int nrhs, const void *const *b, void *const *x, double rel_tol,
+                      double inner_tol, int max_inner, int max_outer, void *ws_hi, void *ws_lo, int *inner_iters,
+                      int *outer_iters, double *rel_res, void *stream, bool reliable)
 {
   int rc = check_mr(lat_lo, nrhs);
   if (rc) return rc;
@@ -664,6 +761,17 @@ int qb200_invert_mixed_mrhs(const qb200_lattice *lat_hi, const qb200_operator *o
   for (int i = 0; i < nrhs; i++) {
     if ((rc = qb200_blas_dot(QB200_F64, n1, b[i], b[i], scal, partials, st))) return rc;
     if ((rc = fetch(&bnorm[i], scal, 1, st))) return rc;
+  }
+  if (reliable) {
+    if (!(inner_tol > 0.0 && inner_tol < 1.0)) return api_fail(QB200_EINVAL, "reliable updates need 0 < inner_tol < 1");
+    int k = 0, nup = 0;
+    if ((rc = mr_reliable(lat_hi, op_hi, lat_lo, op_lo, nrhs, b, x, rel_tol, inner_tol, max_inner, max_outer, r, tmp,
+                          partials, scal, L, bnorm, &k, &nup, rel, st)))
+      return rc;
+    if (inner_iters) *inner_iters = k;
+    if (outer_iters) *outer_iters = nup;
+    for (int i = 0; i < nrhs; i++) rel_res[i] = rel[i];
+    return QB200_OK;
   }
   // r_lo: the scaled true residuals in the low precision; rhs_lo = Mhat^dag r_lo
   void *r_lo = L.v[5];
@@ -704,6 +812,25 @@ int qb200_invert_mixed_mrhs(const qb200_lattice *lat_hi, const qb200_operator *o
   if (outer_iters) *outer_iters = outer;
   for (int i = 0; i < nrhs; i++) rel_res[i] = rel[i];
   return QB200_OK;
+}
+
+int qb200_invert_mixed_mrhs(const qb200_lattice *lat_hi, const qb200_operator *op_hi, const qb200_lattice *lat_lo,
+                            const qb200_operator *op_lo, int nrhs, const void *const *b, void *const *x,
+                            double rel_tol, double inner_tol, int max_inner, int max_outer, void *ws_hi, void *ws_lo,
+                            int *inner_iters, int *outer_iters, double *rel_res, void *stream)
+{
+  return mixed_mrhs(lat_hi, op_hi, lat_lo, op_lo, nrhs, b, x, rel_tol, inner_tol, max_inner, max_outer, ws_hi, ws_lo,
+                    inner_iters, outer_iters, rel_res, stream, false);
+}
+
+int qb200_invert_reliable_mrhs(const qb200_lattice *lat_hi, const qb200_operator *op_hi,
+                               const qb200_lattice *lat_lo, const qb200_operator *op_lo, int nrhs,
+                               const void *const *b, void *const *x, double rel_tol, double delta, int max_iter,
+                               int max_updates, void *ws_hi, void *ws_lo, int *iters, int *updates, double *rel_res,
+                               void *stream)
+{
+  return mixed_mrhs(lat_hi, op_hi, lat_lo, op_lo, nrhs, b, x, rel_tol, delta, max_iter, max_updates, ws_hi, ws_lo,
+                    iters, updates, rel_res, stream, true);
 }
 
 } // extern "C"

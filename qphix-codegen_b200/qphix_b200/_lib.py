@@ -117,6 +117,7 @@ SIGNATURES.update({
     "qb200_schur_apply_mrhs": [_LAT, _I, _OP, _I, _P, _P, _P, _P],
     "qb200_invert_cg_mrhs": [_LAT, _I, _OP, _P, _P, _D, _I, _P, _IP, _DP, _P],
     "qb200_invert_mixed_mrhs": [_LAT, _OP, _LAT, _OP, _I, _PP, _PP, _D, _D, _I, _I, _P, _P, _IP, _IP, _DP, _P],
+    "qb200_invert_reliable_mrhs": [_LAT, _OP, _LAT, _OP, _I, _PP, _PP, _D, _D, _I, _I, _P, _P, _IP, _IP, _DP, _P],
 })
 INFO.update({
     "qb200_mrhs_spinor_elems": ([_LAT, _I], _LL),

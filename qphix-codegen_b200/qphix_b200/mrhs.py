@@ -84,9 +84,14 @@ def cg(op: EvenOddOperator, nrhs, b, x=None, tol=1e-10, max_iter=10000):
 
 
 def mixed_solve(op_hi: EvenOddOperator, op_lo: EvenOddOperator, bs, tol=1e-10, inner_tol=1e-2, max_inner=10000,
-                max_outer=50):
-    """Solve Mhat x_i = b_i (FP64 single-layout b_i) for all i with the
-    corrections of all right-hand sides solved together in low precision."""
+                max_outer=50, solver="cg"):
+    """Solve Mhat x_i = b_i (FP64 single-layout b_i) for all i, iterating all
+    right-hand sides together in low precision.  solver "cg": defect
+    correction, each correction solved to inner_tol; "cg_reliable": one CG
+    with FP64 reliable updates whenever the residuals have fallen by
+    inner_tol (max_inner iterations, max_outer updates)."""
+    if solver not in ("cg", "cg_reliable"):
+        raise ValueError("unknown solver %r" % solver)
     L = _lib.lib()
     nrhs = len(bs)
     lo = ctypes.c_longlong(0)
@@ -97,8 +102,8 @@ def mixed_solve(op_hi: EvenOddOperator, op_lo: EvenOddOperator, bs, tol=1e-10, i
     xs = [torch.zeros_like(b) for b in bs]
     ii, oo = ctypes.c_int(0), ctypes.c_int(0)
     rel = (ctypes.c_double * nrhs)()
-    _lib.check(L.qb200_invert_mixed_mrhs(ctypes.byref(op_hi.lat), ctypes.byref(op_hi.op), ctypes.byref(op_lo.lat),
-                                         ctypes.byref(op_lo.op), nrhs, _ptrs(bs), _ptrs(xs), tol, inner_tol,
-                                         max_inner, max_outer, ws_hi.data_ptr(), ws_lo.data_ptr(), ctypes.byref(ii),
-                                         ctypes.byref(oo), rel, _stream()))
+    fn = L.qb200_invert_mixed_mrhs if solver == "cg" else L.qb200_invert_reliable_mrhs
+    _lib.check(fn(ctypes.byref(op_hi.lat), ctypes.byref(op_hi.op), ctypes.byref(op_lo.lat), ctypes.byref(op_lo.op),
+                  nrhs, _ptrs(bs), _ptrs(xs), tol, inner_tol, max_inner, max_outer, ws_hi.data_ptr(),
+                  ws_lo.data_ptr(), ctypes.byref(ii), ctypes.byref(oo), rel, _stream()))
     return xs, {"inner_iters": ii.value, "outer_iters": oo.value, "rel_res": list(rel)}

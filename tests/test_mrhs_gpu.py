@@ -76,3 +76,25 @@ def test_mrhs_cg_and_mixed_fp16(cuda):
         mx = H.oracle_schur(g, family, ff, p, x.cpu().numpy())
         assert np.linalg.norm(ff["b"] - mx) / np.linalg.norm(ff["b"]) < 2e-10
     print(info)
+
+
+@pytest.mark.parametrize("lo,nrhs", [(F16, 4), (F16, 8), (F32, 2)])
+@pytest.mark.parametrize("family", ["clover", "tm"])
+def test_mrhs_reliable_updates(cuda, lo, nrhs, family):
+    """Multi-RHS CG with FP64 reliable updates: every solution to 1e-10
+    against the oracle, in no more iterations than defect correction."""
+    g = Geometry(8, 8, 8, 8, soalen=4, veclen=8, ftype=F64, compress12=True, t_boundary=-1.0)
+    f, p = H.eo_setup(g, family)
+    op64 = _ops(g, family, f, p, cuda)
+    glo = g.with_(ftype=lo)
+    oplo = _ops(glo, family, f, p, cuda, dtype=glo.dtype)
+    rng = np.random.default_rng(9 + nrhs)
+    bs = [torch.from_numpy(rng.normal(size=g.spinor_elems)).to(cuda) for _ in range(nrhs)]
+    xs, info = mrhs.mixed_solve(op64, oplo, bs, tol=1e-10, inner_tol=1e-2, solver="cg_reliable")
+    assert max(info["rel_res"]) <= 1e-10, info
+    for b, x in zip(bs, xs):
+        ff = dict(f, b=b.cpu().numpy())
+        mx = H.oracle_schur(g, family, ff, p, x.cpu().numpy())
+        assert np.linalg.norm(ff["b"] - mx) / np.linalg.norm(ff["b"]) < 2e-10
+    _, dc = mrhs.mixed_solve(op64, oplo, bs, tol=1e-10, inner_tol=1e-2)
+    assert info["inner_iters"] <= dc["inner_iters"] + 5, (info, dc)
