@@ -90,7 +90,7 @@ class ClockSampler:
                 self.reasons |= self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
             except Exception:
                 pass
-            time.sleep(0.02)
+            time.sleep(0.002)
 
     def __enter__(self):
         if self.nv is not None:
