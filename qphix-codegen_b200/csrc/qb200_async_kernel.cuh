@@ -54,7 +54,9 @@ template <typename FT, int S, bool COMP12> struct AsyncCfg {
   static constexpr int LKB = R * 6 * S * (int)sizeof(elem_t<FT>);    // link slab bytes
   static constexpr int LKS = St::stride(R * 6);
   static constexpr int HOP = St::G * (St::SP + LKS);                 // one hop's staged bytes
-  static constexpr int XOFF = (2 * HOP > St::G * St::CL) ? 2 * HOP : St::G * St::CL;
+  static constexpr int FCL = St::G * St::stride(72);  // staged FullCloverBlock halves
+  static constexpr int XOFF = (2 * HOP > St::G * St::CL) ? (2 * HOP > FCL ? 2 * HOP : FCL)
+                                                         : (St::G * St::CL > FCL ? St::G * St::CL : FCL);
   // 16-bit storage: an x region, staged once for both x hops, holds blocks
   // blk0-1 .. blk0+G, the first block of the warp's first row and the last
   // block of its last row -- every x neighbour of the warp's sites, also
@@ -260,6 +262,17 @@ __device__ __forceinline__ void async_body(const KArgs<FT> &a, const GeoDev &g, 
           res[sp][c].im = fma(r, ch[sp][c].re, res[sp][c].im);
         }
       }
+    } else if (FAM == FAM_TMCLOV) {
+      staged_full_clover<FT, S>(a, w, ch, res);
+#pragma unroll
+      for (int sp = 0; sp < 4; sp++) {
+        const C r = (((p.isPlus != 0) != (sp >= 2)) ? (C)1 : (C)-1) * p.rho;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          res[sp][c].re = fma(-r, ch[sp][c].im, res[sp][c].re);
+          res[sp][c].im = fma(r, ch[sp][c].re, res[sp][c].im);
+        }
+      }
     } else {
       ach_pre<FT, FAM>(a, p, w.tile, w.lane, S, ch, res);
     }
@@ -272,6 +285,7 @@ __device__ __forceinline__ void async_body(const KArgs<FT> &a, const GeoDev &g, 
       for (int c = 0; c < 3; c++) acc[sp][c] = mk<C>(0, 0);
     async_hops<FT, S, COMP12>(a, g, p, s, obase, w, acc);
     if (FAM == FAM_CLOVER) staged_clover<FT, S>(a, w, acc, res);
+    else if (FAM == FAM_TMCLOV) staged_full_clover<FT, S>(a, w, acc, res);
     else plain_post<FT, FAM>(a, p, w.tile, w.lane, S, acc, res);
   }
   store_spinor_sm<FT, S>(w.buf + (w.ln / S) * St::SP, w.lane, res);

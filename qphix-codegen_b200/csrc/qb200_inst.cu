@@ -49,7 +49,7 @@ cudaError_t go(const KArgs<FT> &a, const GeoDev &g, const OpDev<typename ftraits
   if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
   if constexpr (QB_ASYNC && !MR && async_layout<FT, S>()) {
     const bool al = (((uintptr_t)a.psi | (uintptr_t)a.out | (uintptr_t)a.gauge) % 16 == 0) &&
-                    (!ACH || (uintptr_t)a.chi % 16 == 0) && (FAM != FAM_CLOVER || (uintptr_t)a.clov % 16 == 0);
+                    (!ACH || (uintptr_t)a.chi % 16 == 0) && ((FAM != FAM_CLOVER && FAM != FAM_TMCLOV) || (uintptr_t)a.clov % 16 == 0);
     if (g.V == S && al) {
       async_site_kernel<FT, S, COMP12, FAM, ACH><<<grid, kThreads, 0, st>>>(a, g, p);
       return cudaGetLastError();
@@ -73,7 +73,7 @@ cudaError_t go(const KArgs<FT> &a, const GeoDev &g, const OpDev<typename ftraits
   // vectors
   if constexpr (!MR && staged_layout<FT, S>()) {
     const bool al = (((uintptr_t)a.psi | (uintptr_t)a.out | (uintptr_t)a.gauge) % 16 == 0) &&
-                    (!ACH || (uintptr_t)a.chi % 16 == 0) && (FAM != FAM_CLOVER || (uintptr_t)a.clov % 16 == 0);
+                    (!ACH || (uintptr_t)a.chi % 16 == 0) && ((FAM != FAM_CLOVER && FAM != FAM_TMCLOV) || (uintptr_t)a.clov % 16 == 0);
     if (g.V == S && al) {
       staged_site_kernel<FT, S, COMP12, FAM, ACH><<<grid, kThreads, 0, st>>>(a, g, p);
       return cudaGetLastError();
@@ -156,7 +156,7 @@ cudaError_t go_batch(const BatchDev<FT> &b, bool vfixed, int grid, int block, cu
     for (int k = 0; k < b.n && al; k++) {
       const KArgs<FT> &x = b.it[k].a;
       al = (((uintptr_t)x.psi | (uintptr_t)x.out | (uintptr_t)x.gauge) % 16 == 0) &&
-           (!ACH || (uintptr_t)x.chi % 16 == 0) && (FAM != FAM_CLOVER || (uintptr_t)x.clov % 16 == 0);
+           (!ACH || (uintptr_t)x.chi % 16 == 0) && ((FAM != FAM_CLOVER && FAM != FAM_TMCLOV) || (uintptr_t)x.clov % 16 == 0);
     }
     if (al) {
       BatchDev<FT> bw = b;

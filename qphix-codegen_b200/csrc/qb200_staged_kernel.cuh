@@ -302,6 +302,41 @@ __device__ __forceinline__ void staged_clover(const KArgs<FT> &a, const WarpCtx 
   }
 }
 
+// res = the FullCloverBlock of the site's tile applied to in (dense 6x6
+// complex per half, full_clover_block's operation order), both halves
+// staged; buf needs Stage::G * Stage::stride(72) bytes
+template <typename FT, int S>
+__device__ __forceinline__ void staged_full_clover(const KArgs<FT> &a, const WarpCtx &w,
+                                                   const cx<comp_t<FT>> (&in)[4][3], cx<comp_t<FT>> (&res)[4][3])
+{
+  typedef comp_t<FT> C;
+  typedef Stage<FT, S> St;
+  constexpr int FCB = 72 * S * (int)sizeof(elem_t<FT>);
+  constexpr int FCS = St::stride(72);
+#pragma unroll
+  for (int blk = 0; blk < 2; blk++) {
+    stage_in<FT, S, FCB, FCS>(a.clov, w.tile * (144LL * S) + blk * 72LL * S, w.buf, w.ln);
+    __syncwarp();
+    const unsigned char *grp = w.buf + (w.ln / S) * FCS;
+#pragma unroll
+    for (int r = 0; r < 6; r++) {
+      C re = 0, im = 0;
+#pragma unroll
+      for (int c = 0; c < 6; c++) {
+        const C ar = sm_ld<FT, S>(grp, (r * 6 + c) * 2 + 0, w.lane);
+        const C ai = sm_ld<FT, S>(grp, (r * 6 + c) * 2 + 1, w.lane);
+        const cx<C> v = in[2 * blk + c / 3][c % 3];
+        re = fma(ar, v.re, re);
+        re = fma(-ai, v.im, re);
+        im = fma(ar, v.im, im);
+        im = fma(ai, v.re, im);
+      }
+      res[2 * blk + r / 3][r % 3] = mk<C>(re, im);
+    }
+    __syncwarp();
+  }
+}
+
 template <typename FT, int S, bool COMP12> struct StagedSmem {
   static constexpr int BYTES = Stage<FT, S>::BUF + Stage<FT, S>::G * Stage<FT, S>::stride((COMP12 ? 2 : 3) * 6);
 };
