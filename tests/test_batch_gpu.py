@@ -82,16 +82,20 @@ def test_batch_rejects_mixed_layouts(cuda):
         batch.BatchedDslash("wilson", "dslash", 1, probs)()
 
 
-def test_batched_ragged_planes(cuda):
-    """planes whose site count is not a multiple of 32 (the staged batched
-    kernel pads each plane to whole warps)"""
+@pytest.mark.parametrize("ft,S,dims", [
+    (F32, 4, [(24, 6, 4, 4), (8, 6, 4, 4), (16, 8, 4, 4)]),
+    (F16, 8, [(48, 6, 4, 4), (16, 6, 4, 4), (48, 2, 4, 4)])])
+def test_batched_ragged_planes(cuda, ft, S, dims):
+    """planes whose site count is not a multiple of 32 (the batched kernels
+    pad each plane to whole warps) and, at 16 bits, rows of three blocks that
+    do not line up with a warp's blocks (the x region)"""
     global DIMS
     saved = DIMS
     try:
-        DIMS = [(24, 6, 4, 4), (8, 6, 4, 4), (16, 8, 4, 4)]
-        for family in ("clover", "tm"):
+        DIMS = dims
+        for family in ("clover", "tm", "tm_clover"):
             for kernel in H.KERNELS:
-                probs, refs = _problems(F32, 4, family, kernel, True, cuda, seed=320)
+                probs, refs = _problems(ft, S, family, kernel, True, cuda, seed=320)
                 op = batch.BatchedDslash(family, kernel, 1, probs)
                 for grid, block in ((0, 128), (2, 128), (5, 64)):
                     for p in probs:
