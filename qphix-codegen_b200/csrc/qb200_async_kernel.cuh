@@ -137,13 +137,16 @@ __device__ __forceinline__ void compute_hop(const KArgs<FT> &a, const GeoDev &g,
   const long long nbase = obase + neighbour_offset<S, D>(g, s, (long long)St::SPB * S, 1, &cross);
   if (cross && !((p.acc_mask >> D) & 1u)) return;
   cx<C> psi[4][3], G[3][3];
+  // FP16 + norm: the neighbour's norm scales the hop's coefficient, not its
+  // 24 components (the hop is linear in psi)
+  C nrm = (C)1;
   if (MU == 0 && A::XREG) {
     int xb, nl;
     x_neighbour<S, D>(g, s, xb, nl);
     // slot of the row's first block, then of the neighbour's block
     int sl = (int)(w.blk - w.blk0) + 1 - s.xcb / S + xb;
     sl = (sl >= 0 && sl < St::G + 2) ? sl : (sl == w.xhead ? St::G + 2 : St::G + 3);
-    load_spinor_sm<FT, S>(w.xr + sl * St::SP, nl, psi);
+    load_spinor_sm_raw<FT, S>(w.xr + sl * St::SP, nl, psi, nrm);
   } else if (MU == 0) {
     const long long nb = nbase / (St::SPB * S);
     const int nl = (int)(nbase - nb * (St::SPB * S));
@@ -151,12 +154,13 @@ __device__ __forceinline__ void compute_hop(const KArgs<FT> &a, const GeoDev &g,
     if (gi >= 0 && gi < St::G) load_spinor_sm<FT, S>(buf + gi * St::SP, nl, psi);
     else load_spinor<FT, S>(a.psi, nbase, psi);
   } else {
-    load_spinor_sm<FT, S>(buf + (w.ln / S) * St::SP, w.lane, psi);
+    load_spinor_sm_raw<FT, S>(buf + (w.ln / S) * St::SP, w.lane, psi, nrm);
   }
   load_link_sm<FT, S, COMP12>(buf + St::G * St::SP + (w.ln / S) * A::LKS, w.lane, G);
   C beta = p.beta[D];
   if (D == 6 && s.t == 0 && p.t_edge_lo) beta *= p.tbound;
   if (D == 7 && s.t == g.nt - 1 && p.t_edge_hi) beta *= p.tbound;
+  if (ftraits<FT>::SPB == 26) beta *= nrm;
   cx<C> b[2][3], ub[2][3];
   const C sigma = p.isPlus ? (C)1 : (C)-1;
   project<C, D>(psi, sigma, b);

@@ -124,6 +124,24 @@ __device__ __forceinline__ void load_spinor_sm(const unsigned char *grp, int lan
   }
 }
 
+// load_spinor_sm without the FP16 + norm scaling: the site's norm is
+// returned in nrm instead (1 for the other storage types)
+template <typename FT, int S>
+__device__ __forceinline__ void load_spinor_sm_raw(const unsigned char *grp, int lane, cx<comp_t<FT>> (&sp)[4][3],
+                                                   comp_t<FT> &nrm)
+{
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      sp[s][c].re = sm_ld<FT, S>(grp, (c * 4 + s) * 2 + 0, lane);
+      sp[s][c].im = sm_ld<FT, S>(grp, (c * 4 + s) * 2 + 1, lane);
+    }
+  nrm = (comp_t<FT>)1;
+  if (ftraits<FT>::SPB == 26)
+    nrm = reinterpret_cast<const float *>(reinterpret_cast<const elem_t<FT> *>(grp) + 24 * S)[lane];
+}
+
 // the inverse of load_spinor_sm, with the norm of store_spinor
 template <typename FT, int S>
 __device__ __forceinline__ void store_spinor_sm(unsigned char *grp, int lane, const cx<comp_t<FT>> (&sp)[4][3])
