@@ -264,6 +264,129 @@ template <int S> struct F16NSiteF {
   }
 };
 
+// Warp tiles of FP16 + norm vectors: a warp moves the 32/S blocks of 32
+// sites (52 bytes per site) between global and shared memory in 16-byte
+// vectors and each lane decodes / encodes its own site there, so the global
+// accesses are whole sectors instead of the 2*S-byte component pieces that
+// one site per thread touches.  Same arithmetic as F16NSiteF.
+template <int S> struct F16NTile {
+  static constexpr int G = 32 / S;  // blocks per tile
+  static constexpr int CH = 52 * S / 16;  // 16-byte vectors per block
+  static constexpr int N = G * CH;        // vectors per tile (104)
+  static constexpr int BYTES = 16 * N;
+  // blocks blk0 .. blk0+G-1 (those below nblk) -> sm
+  static __device__ __forceinline__ void load(const __half *f, long long blk0, long long nblk, unsigned char *sm,
+                                              int ln)
+  {
+    const uint4 *src = reinterpret_cast<const uint4 *>(f) + blk0 * CH;
+    const long long avail = (nblk - blk0) * CH;
+#pragma unroll
+    for (int r = 0; r < (N + 31) / 32; r++) {
+      const int j = ln + 32 * r;
+      if (j < N && j < avail) reinterpret_cast<uint4 *>(sm)[j] = __ldg(src + j);
+    }
+  }
+  static __device__ __forceinline__ void store(__half *f, long long blk0, long long nblk, const unsigned char *sm,
+                                               int ln)
+  {
+    uint4 *dst = reinterpret_cast<uint4 *>(f) + blk0 * CH;
+    const long long avail = (nblk - blk0) * CH;
+#pragma unroll
+    for (int r = 0; r < (N + 31) / 32; r++) {
+      const int j = ln + 32 * r;
+      if (j < N && j < avail) dst[j] = reinterpret_cast<const uint4 *>(sm)[j];
+    }
+  }
+  // lane ln's site of the tile in sm
+  static __device__ __forceinline__ void get(const unsigned char *sm, int ln, float (&v)[24])
+  {
+    const __half *b = reinterpret_cast<const __half *>(sm + (ln / S) * 52 * S);
+    const int l = ln % S;
+    const float nrm = reinterpret_cast<const float *>(b + 24 * S)[l];
+#pragma unroll
+    for (int k = 0; k < 24; k++) v[k] = __half2float(b[k * S + l]) * nrm;
+  }
+  static __device__ __forceinline__ void put(unsigned char *sm, int ln, const float (&v)[24])
+  {
+    __half *b = reinterpret_cast<__half *>(sm + (ln / S) * 52 * S);
+    const int l = ln % S;
+    float m = 0.f;
+#pragma unroll
+    for (int k = 0; k < 24; k++) m = fmaxf(m, fabsf(v[k]));
+    const float nrm = m > 0.f ? m : 1.0f;
+    reinterpret_cast<float *>(b + 24 * S)[l] = nrm;
+    const float inv = 1.0f / nrm;
+#pragma unroll
+    for (int k = 0; k < 24; k++) b[k * S + l] = __float2half_rn(v[k] * inv);
+  }
+};
+
+// y = a x + b y over nblk blocks (16-byte aligned fields), 256 threads
+template <int S>
+__global__ void __launch_bounds__(256) axpby_f16n_tile_kernel(long long nblk, ScalarRef a,
+                                                              const __half *__restrict__ x, ScalarRef b,
+                                                              __half *__restrict__ y)
+{
+  typedef F16NTile<S> T;
+  __shared__ __align__(16) unsigned char sm[8][2][T::BYTES];
+  const float av = (float)a.get(), bv = (float)b.get();
+  const int wp = threadIdx.x >> 5, ln = threadIdx.x & 31;
+  const long long ntile = (nblk + T::G - 1) / T::G;
+  for (long long t = blockIdx.x * 8LL + wp; t < ntile; t += gridDim.x * 8LL) {
+    const long long blk0 = t * T::G;
+    T::load(x, blk0, nblk, sm[wp][0], ln);
+    T::load(y, blk0, nblk, sm[wp][1], ln);
+    __syncwarp();
+    if (blk0 + ln / S < nblk) {
+      float vx[24], vy[24];
+      T::get(sm[wp][0], ln, vx);
+      T::get(sm[wp][1], ln, vy);
+#pragma unroll
+      for (int k = 0; k < 24; k++) vy[k] = av * vx[k] + bv * vy[k];
+      T::put(sm[wp][1], ln, vy);
+    }
+    __syncwarp();
+    T::store(y, blk0, nblk, sm[wp][1], ln);
+    __syncwarp();
+  }
+}
+
+// real dot partials over nblk blocks (16-byte aligned fields); each site's
+// 24 terms in FP32, the sites in FP64; kRedThreads threads
+template <int S>
+__global__ void __launch_bounds__(kRedThreads) dot_f16n_tile_kernel(long long nblk, const __half *__restrict__ x,
+                                                                    const __half *__restrict__ y,
+                                                                    double *__restrict__ partials)
+{
+  typedef F16NTile<S> T;
+  constexpr int W = kRedThreads / 32;
+  __shared__ __align__(16) unsigned char sm[W][2][T::BYTES];
+  const int wp = threadIdx.x >> 5, ln = threadIdx.x & 31;
+  const long long ntile = (nblk + T::G - 1) / T::G;
+  double re = 0.0, im = 0.0;
+  for (long long t = blockIdx.x * (long long)W + wp; t < ntile; t += (long long)gridDim.x * W) {
+    const long long blk0 = t * T::G;
+    T::load(x, blk0, nblk, sm[wp][0], ln);
+    T::load(y, blk0, nblk, sm[wp][1], ln);
+    __syncwarp();
+    if (blk0 + ln / S < nblk) {
+      float vx[24], vy[24];
+      T::get(sm[wp][0], ln, vx);
+      T::get(sm[wp][1], ln, vy);
+      float sr = 0.f;
+#pragma unroll
+      for (int k = 0; k < 24; k++) sr += vx[k] * vy[k];
+      re += (double)sr;
+    }
+    __syncwarp();
+  }
+  block_sum2(re, im);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = re;
+    partials[kRedBlocks + blockIdx.x] = im;
+  }
+}
+
 // y = a x + b y
 template <int S>
 __global__ void __launch_bounds__(256) axpby_f16n_kernel(long long nsl, ScalarRef a, const __half *__restrict__ x,

@@ -9,6 +9,8 @@
 //   Mhat psi = A_oo psi - beta^2 D_oe A_ee^-1 D_eo psi
 // (codegen/dslash_common.cc:1729-1826 and :1830-1932 for the two halves).
 // No entry point allocates device memory: the caller passes a workspace.
+#include <algorithm>
+#include <cstdint>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -245,6 +247,13 @@ cudaError_t axpby(const VS &v, ScalarRef a, const void *x, ScalarRef b, void *y,
 {
   if (v.ft != QB200_F16N) return axpby(v.ft, v.n, a, x, b, y, st);
   const long long nsl = v.site_lanes();
+  if ((((uintptr_t)x | (uintptr_t)y) % 16) == 0) {
+    // warp tiles of 32 sites, 8 per block of 256 threads
+    const long long nblk = nsl / v.S, ntile = (nsl + 31) / 32;
+    const int grid = (int)std::min<long long>((ntile + 7) / 8, 148LL * 16);
+    QB_F16N_S(v.S, (axpby_f16n_tile_kernel<SS><<<grid, 256, 0, st>>>(nblk, a, (const __half *)x, b, (__half *)y)));
+    return cudaGetLastError();
+  }
   QB_F16N_S(v.S, (axpby_f16n_kernel<SS><<<grid_for(nsl), 256, 0, st>>>(nsl, a, (const __half *)x, b, (__half *)y)));
   return cudaGetLastError();
 }
@@ -262,7 +271,10 @@ cudaError_t f16n_dot(const VS &v, bool cplx, const void *x, const void *y, doubl
                      cudaStream_t st)
 {
   const long long nsl = v.site_lanes();
-  if (cplx) {
+  if (!cplx && (((uintptr_t)x | (uintptr_t)y) % 16) == 0) {
+    QB_F16N_S(v.S, (dot_f16n_tile_kernel<SS><<<kRedBlocks, kRedThreads, 0, st>>>(nsl / v.S, (const __half *)x,
+                                                                                  (const __half *)y, partials)));
+  } else if (cplx) {
     QB_F16N_S(v.S, (dot_f16n_partial_kernel<SS, true><<<kRedBlocks, kRedThreads, 0, st>>>(
                         nsl, (const __half *)x, (const __half *)y, partials)));
   } else {
