@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bound of the CPU baseline sample")
     ap.add_argument("--no-extras", action="store_true", help="skip the multi-RHS and solver measurements")
-    ap.add_argument("--only", choices=["mrhs", "force", "batch", "solve", "tm", "solve_tm"],
+    ap.add_argument("--only", choices=["mrhs", "force", "batch", "solve", "tm", "solve_tm", "solve_tm_clover"],
                     help="run one secondary measurement alone (on --dims) and print its JSON line")
     return ap.parse_args()
 
@@ -61,7 +61,7 @@ def bytes_per_site(ft_bytes=4, rows=2):
 
 
 # ---------------------------------------------------------------------------
-# clocks during the timed region (NVML, sampled every 20 ms)
+# clocks during the timed region (NVML, sampled every 2 ms)
 
 class ClockSampler:
     REASONS = {
@@ -103,12 +103,16 @@ class ClockSampler:
             self._stop.set()
             self.t.join()
 
-    def summary(self):
+    def summary(self, other=None):
+        """median SM clock, max clock, sample count and active throttle
+        reasons; other: a second sampler whose samples are merged in"""
         if self.nv is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"]}
-        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
-                "sm_max_mhz": self.max_mhz, "samples": len(self.samples),
-                "reasons": [k for k, v in self.REASONS.items() if self.reasons & v]}
+        smp = list(self.samples) + (list(other.samples) if other is not None else [])
+        rs = self.reasons | (other.reasons if other is not None else 0)
+        return {"sm_mhz": statistics.median(smp) if smp else None,
+                "sm_max_mhz": self.max_mhz, "samples": len(smp),
+                "reasons": [k for k, v in self.REASONS.items() if rs & v]}
 
 
 def measured_peak():
@@ -160,14 +164,19 @@ def pick_reference_lib():
     return None
 
 
-def run_reference_cpu(dims, steps, warmup, seconds, fields_gpu=None, g_gpu=None):
-    """Time the reference kernels on the host; returns a dict."""
+def run_reference_cpu(dims, steps, warmup, seconds, fields_gpu=None, g_gpu=None, name=None, kernel="achimbdpsi",
+                      flop_site=None):
+    """Time the reference kernels (library `name`, default the best the host
+    runs) on the host for the clover `kernel` ("achimbdpsi", or "dslash":
+    the plain clov_dslash with the clover field as given, A^-1 for the
+    inverse-clover variant); returns a dict."""
     import oracle as O
     from qphix_b200 import layout
     from qphix_b200.lattice import Geometry
-    name = pick_reference_lib()
-    if name is None:
+    name = name or pick_reference_lib()
+    if name is None or not O.ref_available(name):
         return {"unavailable": "reference kernels not built (python oracle/ref_build.py)"}
+    flop_site = flop_site or FLOP_SITE
     info = O.ref_info(name)
     g = Geometry(*dims, soalen=info["soalen"], veclen=info["veclen"], compress12=True, t_boundary=-1.0)
     if fields_gpu is not None:
@@ -188,7 +197,7 @@ def run_reference_cpu(dims, steps, warmup, seconds, fields_gpu=None, g_gpu=None)
     out = O.aligned(np.zeros(g.spinor_elems, dtype=np.float32))
     prm = O.make_params(**PARAMS)
     nthreads = os.cpu_count() or 1
-    call = lambda: O.ref_dslash(name, g, "clover", "achimbdpsi", 1, 0, A["psi"], A["gauge"], chi=A["chi"],
+    call = lambda: O.ref_dslash(name, g, "clover", kernel, 1, 0, A["psi"], A["gauge"], chi=A["chi"],
                                 clover=A["clover"], params=prm, out=out, nthreads=nthreads)
     for _ in range(max(1, warmup)):
         call()
@@ -201,9 +210,10 @@ def run_reference_cpu(dims, steps, warmup, seconds, fields_gpu=None, g_gpu=None)
         if time.perf_counter() - t_start > seconds:
             break
     per = sum(times) / len(times)
-    gflops = FLOP_SITE * g.vol_cb / per / 1e9
+    gflops = flop_site * g.vol_cb / per / 1e9
+    wl = WORKLOAD if kernel == "achimbdpsi" else "clov_dslash_plus (A^-1) 32^3x64 FP32 compress12"
     return {"value": gflops, "unit": "GFLOP/s", "cores": nthreads, "kind": "reference",
-            "sample": "%d full-lattice calls of %s on %s (%s)" % (len(times), WORKLOAD, "x".join(map(str, dims)), name),
+            "sample": "%d full-lattice calls of %s on %s (%s)" % (len(times), wl, "x".join(map(str, dims)), name),
             "ms_per_step": per * 1e3, "lib": name, "out": out}
 
 
@@ -330,17 +340,22 @@ def bench_solve(dims, dev, nrhs=8, kappa=0.16):
     return out
 
 
-def bench_solve_tm(dev, dims=(48, 48, 48, 96), kappa=0.16, mu=0.01):
-    """Even-odd twisted-mass system at 48^3x96, M = 1/(2 kappa) (1 + i mu~
-    gamma5) - D/2 with mu~ = 2 kappa mu (in the operator's convention alpha =
-    1/(2 kappa), mu = mu~ and muinv = alpha / (alpha^2 + mu^2) with the
-    untwisted mu; hopping coefficient 1/2), solved for one Gaussian source to |b - Mhat x|/|b| <=
+def bench_solve_tm(dev, dims=(48, 48, 48, 96), kappa=0.16, mu=0.01, family="tm"):
+    """Even-odd twisted-mass (family "tm") or twisted-mass clover ("tm_clover")
+    system at 48^3x96, solved for one Gaussian source to |b - Mhat x|/|b| <=
     1e-10 by (a) FP64 CG on Mhat^dag Mhat, (b) FP32 CG corrected in FP64,
     (c) FP16 + per-site norm CG corrected in FP64 (the configuration's
-    storage), (d) one FP16 + per-site norm CG with FP64 reliable updates
-    (the speed-ups are those of (d)).  The residual of every solution is
-    recomputed with the FP64 operator.  Each path runs once untimed on a loose tolerance, then three
-    times; the median is reported."""
+    storage), (d) one FP16 + per-site norm CG with FP64 reliable updates (the
+    speed-ups are those of (d)).  Twisted mass: M = 1/(2 kappa) (1 + i mu~
+    gamma5) - D/2 with mu~ = 2 kappa mu (operator convention alpha = 1/(2
+    kappa), mu = mu~ and muinv = alpha / (alpha^2 + mu^2) with the untwisted
+    mu; hopping coefficient 1/2).  Twisted-mass clover: the dense
+    FullCloverBlock F = I + 0.1 M + i mu~ gamma5 per block (M a seeded
+    complex Gaussian 6x6 of unit Frobenius norm; gamma5 = +1 on the upper,
+    -1 on the lower block), F_oo on the target checkerboard and F_ee^-1 on
+    the other, hopping coefficient kappa.  The residual of every solution is
+    recomputed with the FP64 operator.  Each path runs once untimed on a
+    loose tolerance, then three times; the median is reported."""
     from qphix_b200 import fields, layout
     from qphix_b200.lattice import F16N, F32, F64, Geometry
     from qphix_b200.solver import EvenOddOperator, mixed_solve
@@ -348,16 +363,36 @@ def bench_solve_tm(dev, dims=(48, 48, 48, 96), kappa=0.16, mu=0.01):
     U = fields.random_gauge(G, seed=177, device=dev)
     gauge = [layout.pack_gauge(G, U, cb, torch.float64) for cb in (0, 1)]
     del U
-    alpha = 1.0 / (2 * kappa)
-    p = dict(coeff_s=0.5, coeff_t_f=0.5, coeff_t_b=0.5, alpha=alpha, mu=mu / alpha,
-             muinv=alpha / (alpha ** 2 + mu ** 2))
     ops_ = {}
-    for ft, dt in ((F64, torch.float64), (F32, torch.float32), (F16N, torch.float16)):
-        ops_[ft] = EvenOddOperator(G.with_(ftype=ft), "tm", gauge=[x.to(dt) for x in gauge], target_cb=1, **p)
+    if family == "tm":
+        alpha = 1.0 / (2 * kappa)
+        p = dict(coeff_s=0.5, coeff_t_f=0.5, coeff_t_b=0.5, alpha=alpha, mu=mu / alpha,
+                 muinv=alpha / (alpha ** 2 + mu ** 2))
+        for ft, dt in ((F64, torch.float64), (F32, torch.float32), (F16N, torch.float16)):
+            ops_[ft] = EvenOddOperator(G.with_(ftype=ft), "tm", gauge=[x.to(dt) for x in gauge], target_cb=1, **p)
+    else:
+        mut = 2 * kappa * mu
+        g5 = torch.tensor([1.0, -1.0], dtype=torch.float64, device=dev).reshape(2, 1, 1)
+        eye = torch.eye(6, dtype=torch.complex128, device=dev)
+        clov, clov_dag = [None, None], [None, None]
+        for cb, seed in ((1, 178), (0, 179)):
+            F = fields.random_full_clover(G, seed=seed, device=dev) + 1j * mut * g5 * eye
+            if cb == 0:
+                F = fields.invert_blocks(F)
+            clov[cb] = layout.pack_full_clover(G, F, torch.float64)
+            clov_dag[cb] = layout.pack_full_clover(G, F.conj().transpose(-1, -2), torch.float64)
+            del F
+        p = dict(coeff_s=kappa, coeff_t_f=kappa, coeff_t_b=kappa, rho=0.0)
+        for ft, dt in ((F64, torch.float64), (F32, torch.float32), (F16N, torch.float16)):
+            ops_[ft] = EvenOddOperator(G.with_(ftype=ft), "tm_clover", gauge=[x.to(dt) for x in gauge],
+                                       clov=[x.to(dt) for x in clov], clov_dag=[x.to(dt) for x in clov_dag],
+                                       target_cb=1, **p)
+        del clov, clov_dag
     del gauge
     b = layout.pack_spinor(G, fields.random_spinor(G, seed=181, device=dev), torch.float64)
-    out = {"lattice": list(dims), "family": "tm", "kappa": kappa, "mu": mu, "tol": 1e-10,
-           "inner_storage": "fp16 + per-site norm (links fp16, 12-real)", "soalen": 8}
+    out = {"lattice": list(dims), "family": family, "kappa": kappa, "mu": mu, "tol": 1e-10,
+           "inner_storage": "fp16 + per-site norm (links%s fp16, 12-real)" % (" and clover" if family != "tm" else ""),
+           "soalen": 8}
     ops_[F64].cg(b, tol=1e-4, max_iter=50)
     mixed_solve(ops_[F64], ops_[F32], b, tol=1e-4, inner_tol=1e-2)
     mixed_solve(ops_[F64], ops_[F16N], b, tol=1e-4, inner_tol=1e-2)
@@ -512,6 +547,79 @@ def bench_tm(dev, dims=(48, 48, 48, 96)):
     return res
 
 
+def site_rel_err(ga, a, gb, b):
+    """max over spinor components of |a - b| / max(|b_i|, rms of b's site):
+    the per-component relative error (a, b: spinor arrays of lattices ga, gb)"""
+    from qphix_b200 import layout
+    ta = layout.unpack_spinor(ga, a.detach().cpu()).reshape(-1, 12)
+    tb = layout.unpack_spinor(gb, b.detach().cpu()).reshape(-1, 12)
+    ra = torch.cat([ta.real, ta.imag], 1).double()
+    rb = torch.cat([tb.real, tb.imag], 1).double()
+    site = (rb.pow(2).sum(1, keepdim=True) / 24).sqrt()
+    den = torch.maximum(rb.abs(), site).clamp_min(1e-300)
+    return float(((ra - rb).abs() / den).max())
+
+
+def cpu_baselines(g, f, dims, seconds, kernel, flop_site=FLOP_SITE):
+    """The reference's AVX512 (or the best the host runs) and scalar builds
+    on all host threads, each on a bounded sample of the same workload and
+    the same inputs as the GPU; the first is the baseline, both are listed
+    with their per-component difference from the GPU result."""
+    from qphix_b200 import ops
+    builds = []
+    names = [n for n in (pick_reference_lib(), "scalar_f32") if n]
+    names = list(dict.fromkeys(names))
+    out = torch.zeros_like(f["psi"])
+    ops.dslash(g, "clover", kernel, 1, 0, f["psi"], out, f["gauge"], chi=f["chi"], clover=f["clover"], **PARAMS)
+    torch.cuda.synchronize()
+    import oracle as O
+    for i, name in enumerate(names):
+        r = run_reference_cpu(dims, 1000, 1, seconds if i == 0 else seconds / 2, fields_gpu=f, g_gpu=g, name=name,
+                              kernel=kernel, flop_site=flop_site)
+        if "unavailable" in r:
+            builds.append({"lib": name, "unavailable": r["unavailable"]})
+            continue
+        info = O.ref_info(r["lib"])
+        gr = g.with_(soalen=info["soalen"], veclen=info["veclen"])
+        b = torch.from_numpy(r["out"][: gr.spinor_elems].copy())
+        e = {k: r[k] for k in ("value", "unit", "cores", "kind", "sample", "lib", "ms_per_step")}
+        e["rel_err_vs_gpu"] = site_rel_err(gr, b, g, out)
+        builds.append(e)
+    ok = [b for b in builds if "value" in b]
+    if not ok:
+        return {"unavailable": "reference kernels not built (python oracle/ref_build.py)"}
+    cpu = {k: ok[0][k] for k in ("value", "unit", "cores", "kind", "sample")}
+    cpu["builds"] = builds
+    return cpu
+
+
+def bench_inverse_clover(g, f, dims, dev, peak, cpu_seconds):
+    """The inverse-clover variant: the plain clov_dslash_plus with A^-1
+    (FP64 block inverses of the clover blocks I + 0.1 H, packed to FP32) on
+    the headline lattice and layout.  1824 flop/site; 864 algorithmic
+    bytes/site (psi 96 + out 96 + 8 links x 48 + clover 288).  The
+    reference's builds run the same call on the same inputs (bounded CPU
+    samples)."""
+    from qphix_b200 import fields, layout, ops
+    A = fields.random_clover(g, seed=1234 + 3, device=dev)
+    Ainv = layout.pack_clover(g, fields.invert_blocks(A))
+    del A
+    fi = dict(f, clover=Ainv)
+    out = torch.zeros_like(f["psi"])
+    stream = torch.cuda.current_stream()
+    ms = _time(lambda: ops.dslash(g, "clover", "dslash", 1, 0, fi["psi"], out, fi["gauge"], clover=fi["clover"],
+                                  **PARAMS), 50, stream)
+    bps = 864
+    res = {"workload": "clov_dslash_plus with A^-1, %s FP32 compress12 SOALEN %d" % ("x".join(map(str, dims)),
+                                                                                  g.soalen),
+           "ms": ms, "gflops": FLOP_SITE * g.vol_cb / (ms * 1e-3) / 1e9,
+           "gbs": bps * g.vol_cb / (ms * 1e-3) / 1e9, "bytes_per_site": bps}
+    res["frac_of_peak"] = res["gbs"] / peak
+    if cpu_seconds:
+        res["cpu_baseline"] = cpu_baselines(g, fi, dims, cpu_seconds, "dslash")
+    return res
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -591,6 +699,26 @@ def b200_arm(args, world, rank, local):
     sites_all = g.vol_cb * world
     gflops = FLOP_SITE * sites_all / (ms_step * 1e-3) / 1e9
     launches_per_step = 1 if world == 1 else 5
+
+    # a window of the same step after the timed region, long enough (about
+    # 0.3 s) for dozens of clock samples even when the timed region is a few
+    # milliseconds; its time x median SM clock ties the two together
+    nwin = max(50, min(20000, int(300.0 / max(ms_step, 1e-3))))
+    w0, w1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index if dev.index is not None else 0) as clkw:
+        barrier()
+        w0.record(stream)
+        for _ in range(nwin):
+            step()
+        w1.record(stream)
+        barrier()
+    win_ms = w0.elapsed_time(w1) / nwin
+    cw = clkw.summary()
+    clock_window = {"steps": nwin, "ms_per_step": win_ms, "sm_mhz": cw.get("sm_mhz"), "samples": cw.get("samples"),
+                    "reasons": cw.get("reasons"),
+                    "ms_x_mhz": win_ms * cw["sm_mhz"] if cw.get("sm_mhz") else None,
+                    "timed_region_ms_x_mhz": (ms_step * clk.summary()["sm_mhz"]
+                                              if clk.summary().get("sm_mhz") else None)}
 
     # roofline of the body kernel: its own events over the same timed region
     bps = bytes_per_site()
@@ -685,24 +813,15 @@ def b200_arm(args, world, rank, local):
                         "copied in and out copied back every step, double-buffered over steps")}
 
     cpu = None
+    inv = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        r = run_reference_cpu(dims, 1000, 1, args.cpu_seconds, fields_gpu=f, g_gpu=g)
-        if "unavailable" in r:
-            cpu = {"unavailable": r["unavailable"]}
-        else:
-            cpu = {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")}
-            # same inputs: the reference result must match the GPU one
-            from qphix_b200 import layout
-            import oracle as O
-            info = O.ref_info(r["lib"])
-            gr = g.with_(soalen=info["soalen"], veclen=info["veclen"])
-            ops.dslash(g, "clover", "achimbdpsi", 1, 0, f["psi"], out, f["gauge"], chi=f["chi"],
-                       clover=f["clover"], **PARAMS)
-            a = layout.unpack_spinor(g, out.cpu())
-            b = layout.unpack_spinor(gr, torch.from_numpy(r["out"][: gr.spinor_elems].copy()))
-            cpu["max_abs_diff_vs_gpu"] = float((a - b).abs().max())
+        cpu = cpu_baselines(g, f, dims, args.cpu_seconds, "achimbdpsi")
+    if rank == 0 and world == 1 and not args.no_extras:
+        inv = bench_inverse_clover(g, f, dims, dev, peak, None if args.no_cpu_baseline else args.cpu_seconds / 2)
 
     extras = {}
+    if inv is not None:
+        extras["inverse_clover"] = inv
     if world == 1 and not args.no_extras:
         extras["mrhs"] = bench_mrhs(g, f, dev)
         extras["solve"] = bench_solve(dims, dev)
@@ -710,6 +829,7 @@ def b200_arm(args, world, rank, local):
         extras["batch"] = bench_batch(dev, peak)
         extras["tm_fp16n"] = bench_tm(dev)
         extras["solve_tm"] = bench_solve_tm(dev)
+        extras["solve_tm_clover"] = bench_solve_tm(dev, family="tm_clover")
 
     if rank == 0:
         line = {
@@ -728,7 +848,9 @@ def b200_arm(args, world, rank, local):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps,
-            "clocks": clk.summary(),
+            "clocks": clk.summary(clkw),
+            "clocks_timed_region": clk.summary(),
+            "clock_window": clock_window,
         }
         line.update(extras)
         print(json.dumps(line))
@@ -752,6 +874,8 @@ def run_only(args):
         r = bench_tm(dev, dims)
     elif args.only == "solve_tm":
         r = bench_solve_tm(dev, dims)
+    elif args.only == "solve_tm_clover":
+        r = bench_solve_tm(dev, dims, family="tm_clover")
     else:
         r = bench_solve(dims, dev)
     print(json.dumps({"only": args.only, "dims": list(dims), "result": r}))

@@ -157,7 +157,7 @@ int qb200_dslash_achimbdpsi_minus_vec(
 
 /* Clover: out = A (D psi), A a Hermitian CloverBlock field (callers pass
  * A^-1 for the even-odd operator).  Replaces
- * QPhiX::clov_dslash_{plus,minus}_vec (clov_dslash_decl.h.j2:5-46). */
+ * QPhiX::clov_dslash_{plus,minus}_vec (clov_dslash_decl.h.j2:7-46). */
 int qb200_clov_dslash_plus_vec(const qb200_lattice *lat, int cb,
                                const void *psi, void *out, const void *gauge,
                                const void *clover,
@@ -175,7 +175,7 @@ int qb200_clov_dslash_minus_vec(const qb200_lattice *lat, int cb,
 
 /* Clover: out = A chi + i rho g5 chi (sign flips for minus) - D psi.
  * Replaces QPhiX::clov_dslash_achimbdpsi_{plus,minus}_vec
- * (clov_dslash_decl.h.j2:48-94; dslash_common.cc:1830-1932). */
+ * (clov_dslash_decl.h.j2:49-94; dslash_common.cc:1830-1932). */
 int qb200_clov_dslash_achimbdpsi_plus_vec(
     const qb200_lattice *lat, int cb, const void *psi, const void *chi,
     void *out, const void *gauge, const void *clover, double coeff_s,
@@ -223,7 +223,7 @@ int qb200_tm_dslash_achimbdpsi_minus_vec(
 
 /* Twisted-mass clover: out = F (D psi), F a dense FullCloverBlock field.
  * Replaces QPhiX::tm_clov_dslash_{plus,minus}_vec
- * (tm_clov_dslash_decl.h.j2; full_clover_term, dslash_common.cc:1188-1232). */
+ * (tm_clov_dslash_decl.h.j2:7-46; full_clover_term, dslash_common.cc:1188-1232). */
 int qb200_tm_clov_dslash_plus_vec(const qb200_lattice *lat, int cb,
                                   const void *psi, void *out,
                                   const void *gauge, const void *full_clover,
@@ -241,7 +241,7 @@ int qb200_tm_clov_dslash_minus_vec(const qb200_lattice *lat, int cb,
 
 /* Twisted-mass clover: out = F chi + i rho g5 chi - D psi.  Replaces
  * QPhiX::tm_clov_dslash_achimbdpsi_{plus,minus}_vec
- * (tm_clov_dslash_decl.h.j2:48-94). */
+ * (tm_clov_dslash_decl.h.j2:49-94). */
 int qb200_tm_clov_dslash_achimbdpsi_plus_vec(
     const qb200_lattice *lat, int cb, const void *psi, const void *chi,
     void *out, const void *gauge, const void *full_clover, double coeff_s,
@@ -278,7 +278,7 @@ int qb200_face_proj_dir_minus(const qb200_lattice *lat, int psi_cb,
  * the clover field to it (codegen/dslash_common.cc:1934-1993).  tbc != 0
  * applies tbc_phases[dir/2].  Replaces QPhiX::face_finish_dir_*,
  * face_clov_finish_dir_*, tm_face_finish_dir_*, tm_clov_face_finish_dir_*
- * (dslash_decl.h.j2:101-115, clov_dslash_decl.h.j2:214-231,
+ * (dslash_decl.h.j2:101-115, clov_dslash_decl.h.j2:96-113,
  * tm_dslash_decl.h.j2:93-109, tm_clov_dslash_decl.h.j2:97-113).
  */
 int qb200_face_finish_dir_plus(const qb200_lattice *lat, int cb,
@@ -368,7 +368,9 @@ int qb200_schur_apply(const qb200_lattice *lat, const qb200_operator *op, int is
  * array's device address (cudaGetSymbolAddress) with that device current;
  * make that first call before any stream capture.  All calls share the one
  * array: calls that overlap on the GPU race and must be serialised by the
- * caller.  The function allocates nothing. */
+ * caller.  The array's address is looked up once per device and kept, so do
+ * not use this entry point across cudaDeviceReset (or any other teardown of
+ * the device's primary context).  The function allocates nothing. */
 #define QB200_NOALLOC_SCRATCH_BYTES (32 << 20)
 int qb200_schur_apply_noalloc(const qb200_lattice *lat, const qb200_operator *op, int isign, const void *in,
                               void *out, void *stream);

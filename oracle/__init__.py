@@ -110,54 +110,70 @@ def liboracle():
         V = ctypes.c_void_p
         I, D = ctypes.c_int, ctypes.c_double
         L.oracle_dslash.argtypes = [LP, I, I, I, I, V, V, V, V, V, ctypes.POINTER(Params)]
+        L.oracle_dslash_out.argtypes = [LP, I, I, I, I, I, V, V, V, V, V, ctypes.POINTER(Params)]
+        L.oracle_spinor_elems_f64.argtypes = [LP]
+        L.oracle_spinor_elems_f64.restype = ctypes.c_longlong
         L.oracle_face_count.argtypes = [LP, I, I]
         L.oracle_face_count.restype = ctypes.c_longlong
         L.oracle_face_pack.argtypes = [LP, I, I, V, V, I, V]
+        L.oracle_face_pack_out.argtypes = [LP, I, I, I, V, V, I, V]
         L.oracle_face_unpack.argtypes = [LP, I, I, I, V, V, V, V, D, D, D, I, I, V, V]
+        L.oracle_face_unpack_out.argtypes = [LP, I, I, I, I, V, V, V, V, D, D, D, I, I, V, V]
         L.oracle_hop_force.argtypes = [LP, I, I, V, V, V, ctypes.POINTER(Params), V]
         _oracle = L
     return _oracle
 
 
-def dslash(g, family, kernel, isign, cb, psi, gauge, chi=None, clover=None, params=None, out=None):
-    """Oracle body kernel; returns out (numpy, storage dtype)."""
+def dslash(g, family, kernel, isign, cb, psi, gauge, chi=None, clover=None, params=None, out=None, fp64_out=False):
+    """Oracle body kernel; returns out (numpy, storage dtype).  fp64_out: the
+    result unrounded, as an FP64 spinor array of the same lattice (layout of
+    g with ftype QB200_F64)."""
     L = liboracle()
     lat = lattice_struct(g)
     p = params if params is not None else make_params()
     if out is None:
-        out = np.zeros(psi.size, dtype=psi.dtype)
-    rc = L.oracle_dslash(ctypes.byref(lat), FAMILY[family], 1 if kernel == "achimbdpsi" else 0,
-                         1 if isign > 0 else -1, cb, _ptr(psi), _ptr(chi), _ptr(gauge), _ptr(clover),
-                         _ptr(out), ctypes.byref(p))
+        if fp64_out:
+            n = L.oracle_spinor_elems_f64(ctypes.byref(lat))
+            out = np.zeros(n, dtype=np.float64)
+        else:
+            out = np.zeros(psi.size, dtype=psi.dtype)
+    rc = L.oracle_dslash_out(ctypes.byref(lat), 1 if fp64_out else g.ftype, FAMILY[family],
+                             1 if kernel == "achimbdpsi" else 0, 1 if isign > 0 else -1, cb, _ptr(psi), _ptr(chi),
+                             _ptr(gauge), _ptr(clover), _ptr(out), ctypes.byref(p))
     if rc:
         raise RuntimeError("oracle_dslash failed: %d" % rc)
     return out
 
 
-def face_pack(g, isign, psi_cb, psi, dir):
+def face_pack(g, isign, psi_cb, psi, dir, fp64_out=False):
+    """Face records of psi towards dir; fp64_out: unrounded, 12 doubles per site."""
     L = liboracle()
     lat = lattice_struct(g)
     n = L.oracle_face_count(ctypes.byref(lat), psi_cb, dir)
-    buf = np.zeros((14 if g.ftype == 3 else 12) * n, dtype=psi.dtype)
+    if fp64_out:
+        buf = np.zeros(12 * n, dtype=np.float64)
+    else:
+        buf = np.zeros((14 if g.ftype == 3 else 12) * n, dtype=psi.dtype)
     scratch = np.zeros(4 * n + 4, dtype=np.int32)
-    rc = L.oracle_face_pack(ctypes.byref(lat), 1 if isign > 0 else -1, psi_cb, _ptr(psi), _ptr(buf), dir,
-                            _ptr(scratch))
+    rc = L.oracle_face_pack_out(ctypes.byref(lat), 1 if fp64_out else g.ftype, 1 if isign > 0 else -1, psi_cb,
+                                _ptr(psi), _ptr(buf), dir, _ptr(scratch))
     if rc:
         raise RuntimeError("oracle_face_pack failed: %d" % rc)
     return buf
 
 
 def face_unpack(g, family, isign, cb, inbuf, gauge, out, dir, beta=1.0, clover=None, mu=0.0, muinv=1.0,
-                tbc=False, tbc_phases=None):
-    """Accumulates into `out` in place (numpy); returns out."""
+                tbc=False, tbc_phases=None, fp64_out=False):
+    """Accumulates into `out` in place (numpy); returns out.  fp64_out: out is
+    an FP64 spinor array (layout of g with ftype QB200_F64), kept unrounded."""
     L = liboracle()
     lat = lattice_struct(g)
     n = L.oracle_face_count(ctypes.byref(lat), cb, dir)
     scratch = np.zeros(4 * n + 4, dtype=np.int32)
     ph = np.asarray(tbc_phases if tbc_phases is not None else [[1.0, 0.0]] * 4, dtype=np.float64).reshape(-1)
-    rc = L.oracle_face_unpack(ctypes.byref(lat), FAMILY[family], 1 if isign > 0 else -1, cb, _ptr(inbuf),
-                              _ptr(gauge), _ptr(out), _ptr(clover), beta, mu, muinv, dir, 1 if tbc else 0,
-                              _ptr(ph), _ptr(scratch))
+    rc = L.oracle_face_unpack_out(ctypes.byref(lat), 1 if fp64_out else g.ftype, FAMILY[family],
+                                  1 if isign > 0 else -1, cb, _ptr(inbuf), _ptr(gauge), _ptr(out), _ptr(clover),
+                                  beta, mu, muinv, dir, 1 if tbc else 0, _ptr(ph), _ptr(scratch))
     if rc:
         raise RuntimeError("oracle_face_unpack failed: %d" % rc)
     return out

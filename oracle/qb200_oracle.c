@@ -381,13 +381,19 @@ static int neighbour(const geo *g, int cb, int d, int xcb, int y, int z,
 /* ------------------------------------------------------------------ */
 /* body kernels                                                         */
 
-int oracle_dslash(const qb200_lattice *lat, int family, int achimbdpsi,
-                  int isign, int cb, const void *psi, const void *chi,
-                  const void *gauge, const void *clov, void *out,
-                  const oracle_params *p)
+/* The body kernels with the result stored in storage type out_ft (same
+ * lattice and tile layout as the inputs): out_ft = QB200_F64 keeps the FP64
+ * result unrounded, the reference against which 16-bit storage is judged. */
+int oracle_dslash_out(const qb200_lattice *lat, int out_ft, int family,
+                      int achimbdpsi, int isign, int cb, const void *psi,
+                      const void *chi, const void *gauge, const void *clov,
+                      void *out, const oracle_params *p)
 {
-  geo g;
+  geo g, go;
   if (make_geo(lat, &g)) return QB200_EINVAL;
+  if (out_ft < QB200_F32 || out_ft > QB200_BF16) return QB200_EINVAL;
+  go = g;
+  go.ft = out_ft;
   if (!psi || !gauge || !out) return QB200_ENULL;
   if (achimbdpsi && !chi) return QB200_ENULL;
   if ((family == FAM_CLOVER || family == FAM_TMCLOV) && !clov) return QB200_ENULL;
@@ -470,9 +476,18 @@ int oracle_dslash(const qb200_lattice *lat, int family, int achimbdpsi,
         memcpy(res, hop, sizeof(res));
       }
     }
-    store_spinor(&g, out, xcb, y, z, t, res);
+    store_spinor(&go, out, xcb, y, z, t, res);
   }
   return QB200_OK;
+}
+
+int oracle_dslash(const qb200_lattice *lat, int family, int achimbdpsi,
+                  int isign, int cb, const void *psi, const void *chi,
+                  const void *gauge, const void *clov, void *out,
+                  const oracle_params *p)
+{
+  return oracle_dslash_out(lat, lat->ftype, family, achimbdpsi, isign, cb, psi,
+                           chi, gauge, clov, out, p);
 }
 
 /* ------------------------------------------------------------------ */
@@ -588,6 +603,14 @@ static long long face_sites(const geo *g, int cb, int mu, int coord, int *fx,
   return n;
 }
 
+/* elements of one checkerboard spinor array of lat with FP64 storage */
+long long oracle_spinor_elems_f64(const qb200_lattice *lat)
+{
+  geo g;
+  if (make_geo(lat, &g)) return -1;
+  return (long long)g.nt * g.Pxyz * 24 * g.S;
+}
+
 long long oracle_face_count(const qb200_lattice *lat, int cb, int dir)
 {
   geo g;
@@ -599,12 +622,16 @@ long long oracle_face_count(const qb200_lattice *lat, int cb, int dir)
 
 /* face_proj_dir: sites of psi (on psi_cb) on the face towards dir, projected
  * with the projector of the opposite direction (dslash.cc:451-454) */
-int oracle_face_pack(const qb200_lattice *lat, int isign, int psi_cb,
-                     const void *psi, void *outbuf, int dir, int *scratch)
+int oracle_face_pack_out(const qb200_lattice *lat, int out_ft, int isign,
+                         int psi_cb, const void *psi, void *outbuf, int dir,
+                         int *scratch)
 {
-  geo g;
+  geo g, go;
   if (make_geo(lat, &g)) return QB200_EINVAL;
   if (dir < 0 || dir > 7) return QB200_EDIR;
+  if (out_ft < QB200_F32 || out_ft > QB200_BF16) return QB200_EINVAL;
+  go = g;
+  go.ft = out_ft;
   int L[4] = {g.nx, g.ny, g.nz, g.nt};
   int mu = dir / 2;
   int coord = (dir & 1) ? L[mu] - 1 : 0;
@@ -616,21 +643,33 @@ int oracle_face_pack(const qb200_lattice *lat, int isign, int psi_cb,
     cplx sp[4][3], b[2][3];
     load_spinor(&g, psi, fx[i], fy[i], fz[i], ft[i], sp);
     project(pidx, sp, b);
-    store_face(&g, outbuf, i, b);
+    store_face(&go, outbuf, i, b);
   }
   return QB200_OK;
 }
 
-/* face_*finish_dir: accumulate the face contribution into out (on cb) */
-int oracle_face_unpack(const qb200_lattice *lat, int family, int isign,
-                       int cb, const void *inbuf, const void *gauge,
-                       void *out, const void *clov, double beta, double mu,
-                       double muinv, int dir, int tbc,
-                       const double *tbc_phases, int *scratch)
+int oracle_face_pack(const qb200_lattice *lat, int isign, int psi_cb,
+                     const void *psi, void *outbuf, int dir, int *scratch)
 {
-  geo g;
+  return oracle_face_pack_out(lat, lat->ftype, isign, psi_cb, psi, outbuf, dir,
+                              scratch);
+}
+
+/* face_*finish_dir: accumulate the face contribution into out (on cb) */
+/* out_ft: storage type of `out` (read and written), e.g. QB200_F64 for an
+ * unrounded result; the other fields are in lat's storage type */
+int oracle_face_unpack_out(const qb200_lattice *lat, int out_ft, int family,
+                           int isign, int cb, const void *inbuf,
+                           const void *gauge, void *out, const void *clov,
+                           double beta, double mu, double muinv, int dir,
+                           int tbc, const double *tbc_phases, int *scratch)
+{
+  geo g, go;
   if (make_geo(lat, &g)) return QB200_EINVAL;
   if (dir < 0 || dir > 7) return QB200_EDIR;
+  if (out_ft < QB200_F32 || out_ft > QB200_BF16) return QB200_EINVAL;
+  go = g;
+  go.ft = out_ft;
   int L[4] = {g.nx, g.ny, g.nz, g.nt};
   int dim = dir / 2, isBack = !(dir & 1);
   int coord = isBack ? 0 : L[dim] - 1;
@@ -644,7 +683,7 @@ int oracle_face_unpack(const qb200_lattice *lat, int family, int isign,
   double b_eff = clover ? beta : -beta;
   for (long long i = 0; i < n; i++) {
     cplx o[4][3], dout[4][3], b[2][3], ub[2][3], G[3][3];
-    load_spinor(&g, out, fx[i], fy[i], fz[i], ft[i], o);
+    load_spinor(&go, out, fx[i], fy[i], fz[i], ft[i], o);
     load_face(&g, inbuf, i, b);
     load_link(&g, gauge, fx[i], fy[i], fz[i], ft[i], dir, G);
     mult_link(G, isBack, b, ub);
@@ -661,9 +700,20 @@ int oracle_face_unpack(const qb200_lattice *lat, int family, int isign,
     } else if (tm) {
       inv_twisted(isPlus, mu, muinv, dout, o, 1);
     }
-    store_spinor(&g, out, fx[i], fy[i], fz[i], ft[i], o);
+    store_spinor(&go, out, fx[i], fy[i], fz[i], ft[i], o);
   }
   return QB200_OK;
+}
+
+int oracle_face_unpack(const qb200_lattice *lat, int family, int isign,
+                       int cb, const void *inbuf, const void *gauge,
+                       void *out, const void *clov, double beta, double mu,
+                       double muinv, int dir, int tbc,
+                       const double *tbc_phases, int *scratch)
+{
+  return oracle_face_unpack_out(lat, lat->ftype, family, isign, cb, inbuf,
+                                gauge, out, clov, beta, mu, muinv, dir, tbc,
+                                tbc_phases, scratch);
 }
 
 int oracle_abi_version(void) { return QB200_ABI_VERSION; }

@@ -16,11 +16,15 @@ Recipe, per configuration (ISA, precision, SOALEN, low precision):
   4. compile wrappers + oracle/ref_driver.cpp into
      oracle/_ref/libqphix_ref_<cfg>.so.
 The reference's CMake/Jinja library build (generate_files.py, the generated
-CMake project) is not used.  Nothing under /root/reference is copied into the
+CMake project) is not used.  Nothing of the reference checkout is copied into the
 repository: generated sources and binaries stay in the git-ignored
-oracle/_ref/.  The GPU box has no /root/reference and uses the prebuilt .so.
+oracle/_ref/.  A machine without the reference sources uses the prebuilt .so.
 
-Usage: python oracle/ref_build.py [cfg ...]   (default: the DEFAULT list)
+The reference checkout is taken from --ref DIR, else from the environment
+variable QPHIX_CODEGEN_REF, else from the mount point this recipe was written
+for (DEFAULT_REF); DIR is the checkout's root (it holds codegen/).
+
+Usage: python oracle/ref_build.py [--ref DIR] [cfg ...]   (default: the DEFAULT list)
 """
 import concurrent.futures as cf
 import os
@@ -30,7 +34,19 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
-REF = "/root/reference/codegen"
+DEFAULT_REF = "/root/reference"
+REF = None  # codegen/ of the reference checkout, set by set_reference()
+
+
+def reference_dir(explicit=None):
+    """The reference checkout's root, or None when its sources are absent."""
+    root = explicit or os.environ.get("QPHIX_CODEGEN_REF") or DEFAULT_REF
+    return root if os.path.isdir(os.path.join(root, "codegen")) else None
+
+
+def set_reference(root):
+    global REF
+    REF = os.path.join(root, "codegen")
 OUT = os.path.join(HERE, "_ref")
 
 # CMakeLists.txt:151-239 define sets (PREF_* and USE_SHUFFLES off everywhere)
@@ -248,9 +264,17 @@ def build(name, jobs=8, opt="-O2"):
 
 
 def main(argv):
-    if not os.path.isdir(REF):
+    argv = list(argv)
+    explicit = None
+    if "--ref" in argv:
+        i = argv.index("--ref")
+        explicit = argv[i + 1]
+        del argv[i:i + 2]
+    root = reference_dir(explicit)
+    if root is None:
         print("reference sources not present; using prebuilt oracle/_ref if any")
         return 0
+    set_reference(root)
     names = argv or DEFAULT
     for n in names:
         print("building", n, "->", build(n), flush=True)

@@ -244,52 +244,30 @@ __device__ __forceinline__ void async_body(const KArgs<FT> &a, const GeoDev &g, 
     stage_xregion<FT, S, COMP12>(a.psi, w.blk0, w.blk0 - 1 + w.xhead, tail, g.Pxyz * g.nt, w.xr, w.ln);
   }
 
-  cx<C> res[4][3];
+  cx<C> acc[4][3];
 #pragma unroll
   for (int sp = 0; sp < 4; sp++)
 #pragma unroll
-    for (int c = 0; c < 3; c++) res[sp][c] = mk<C>(0, 0);
+    for (int c = 0; c < 3; c++) acc[sp][c] = mk<C>(0, 0);
+  async_hops<FT, S, COMP12>(a, g, p, s, obase, w, acc);
+  cx<C> res[4][3];
   if (ACH) {
+    // the hops (subtracted: beta negated by the host), then + A.chi
     cx<C> ch[4][3];
     stage_in<FT, S, A::SPB, St::SP>(a.chi, w.own, w.buf, w.ln);
     __syncwarp();
     load_spinor_sm<FT, S>(w.buf + (w.ln / S) * St::SP, w.lane, ch);
     __syncwarp();
-    if (FAM == FAM_CLOVER) {
-      staged_clover<FT, S>(a, w, ch, res);
-#pragma unroll
-      for (int sp = 0; sp < 4; sp++) {
-        const C r = (((p.isPlus != 0) != (sp >= 2)) ? (C)1 : (C)-1) * p.rho;
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-          res[sp][c].re = fma(-r, ch[sp][c].im, res[sp][c].re);
-          res[sp][c].im = fma(r, ch[sp][c].re, res[sp][c].im);
-        }
-      }
-    } else if (FAM == FAM_TMCLOV) {
-      staged_full_clover<FT, S>(a, w, ch, res);
-#pragma unroll
-      for (int sp = 0; sp < 4; sp++) {
-        const C r = (((p.isPlus != 0) != (sp >= 2)) ? (C)1 : (C)-1) * p.rho;
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-          res[sp][c].re = fma(-r, ch[sp][c].im, res[sp][c].re);
-          res[sp][c].im = fma(r, ch[sp][c].re, res[sp][c].im);
-        }
-      }
-    } else {
-      ach_pre<FT, FAM>(a, p, w.tile, w.lane, S, ch, res);
-    }
-    async_hops<FT, S, COMP12>(a, g, p, s, obase, w, res);
-  } else {
-    cx<C> acc[4][3];
+    if (FAM == FAM_CLOVER) staged_clover<FT, S, MODE_ADD, true>(a, w, p.isPlus, p.rho, ch, acc);
+    else if (FAM == FAM_TMCLOV) staged_full_clover<FT, S, MODE_ADD, true>(a, w, p.isPlus, p.rho, ch, acc);
+    else ach_finish<FT, FAM>(a, p, w.tile, w.lane, S, ch, acc);
 #pragma unroll
     for (int sp = 0; sp < 4; sp++)
 #pragma unroll
-      for (int c = 0; c < 3; c++) acc[sp][c] = mk<C>(0, 0);
-    async_hops<FT, S, COMP12>(a, g, p, s, obase, w, acc);
-    if (FAM == FAM_CLOVER) staged_clover<FT, S>(a, w, acc, res);
-    else if (FAM == FAM_TMCLOV) staged_full_clover<FT, S>(a, w, acc, res);
+      for (int c = 0; c < 3; c++) res[sp][c] = acc[sp][c];
+  } else {
+    if (FAM == FAM_CLOVER) staged_clover<FT, S, MODE_SET, false>(a, w, p.isPlus, (C)0, acc, res);
+    else if (FAM == FAM_TMCLOV) staged_full_clover<FT, S, MODE_SET, false>(a, w, p.isPlus, (C)0, acc, res);
     else plain_post<FT, FAM>(a, p, w.tile, w.lane, S, acc, res);
   }
   store_spinor_sm<FT, S>(w.buf + (w.ln / S) * St::SP, w.lane, res);

@@ -437,12 +437,120 @@ __device__ __forceinline__ void recons(const cx<C> (&ub)[2][3], C beta, C tau, c
 // ---------------------------------------------------------------------
 // clover-type terms
 
-// res[block rows] (+)= A in, A the Hermitian CloverBlock block `blk`
-// (dslash_common.cc:1098-1186).  base = tile*72*V + lane.
-template <typename FT, bool ACC>
+// Clover arithmetic, shared by every kernel (the same operations in the same
+// order everywhere, so that all kernels give the same bits).
+//
+// Row r of a 6x6 block is summed in two chains -- for the Hermitian
+// CloverBlock the diagonal and lower-triangle terms (c < r) in one and the
+// upper-triangle terms (c > r) in the other, for the dense FullCloverBlock
+// columns 0-2 and 3-5 -- which are added at the end.  Shorter chains round
+// less than one running sum; it matters in A.chi - b.D.psi, where the clover
+// term and the hops can cancel to a result several times smaller than both.
+// MODE_SET: out = row; MODE_ADD: out = out + row (one more rounding).  RHO:
+// the row first gets + i rhob in[r] (the i rho g5 chi term of the
+// achimbdpsi form, rhob = +/- rho per block, dslash_common.cc:1873-1906).
+enum { MODE_SET = 0, MODE_ADD = 1 };
+
+// the Hermitian block `blk` from its packed elements: dg[6] real diagonal,
+// od[r(r-1)/2+c] = A[r][c] for r > c, A[c][r] = conj(A[r][c])
+// (dslash_common.cc:1098-1186)
+template <typename C, int MODE, bool RHO>
+__device__ __forceinline__ void herm_apply(const C (&dg)[6], const cx<C> (&od)[15], int blk, C rhob,
+                                           const cx<C> (&in)[4][3], cx<C> (&out)[4][3])
+{
+#pragma unroll
+  for (int r = 0; r < 6; r++) {
+    const cx<C> v = in[2 * blk + r / 3][r % 3];
+    C re1 = dg[r] * v.re, im1 = dg[r] * v.im;
+    C re2 = 0, im2 = 0;
+#pragma unroll
+    for (int c = 0; c < 6; c++) {
+      if (c == r) continue;
+      const cx<C> w = in[2 * blk + c / 3][c % 3];
+      if (c < r) { // A[r][c] = od[r(r-1)/2+c]
+        const cx<C> a = od[r * (r - 1) / 2 + c];
+        re1 = fma(a.re, w.re, re1);
+        re1 = fma(-a.im, w.im, re1);
+        im1 = fma(a.re, w.im, im1);
+        im1 = fma(a.im, w.re, im1);
+      } else { // A[r][c] = conj(od[c(c-1)/2+r])
+        const cx<C> a = od[c * (c - 1) / 2 + r];
+        re2 = fma(a.re, w.re, re2);
+        re2 = fma(a.im, w.im, re2);
+        im2 = fma(a.re, w.im, im2);
+        im2 = fma(-a.im, w.re, im2);
+      }
+    }
+    C re = re1 + re2, im = im1 + im2;
+    if (RHO) {
+      re = fma(-rhob, v.im, re);
+      im = fma(rhob, v.re, im);
+    }
+    cx<C> &o = out[2 * blk + r / 3][r % 3];
+    if (MODE == MODE_ADD) {
+      o.re = o.re + re;
+      o.im = o.im + im;
+    } else {
+      o.re = re;
+      o.im = im;
+    }
+  }
+}
+
+// the dense block `blk`; ld(r, c) returns element (r, c)
+// (dslash_common.cc:1188-1232)
+template <typename C, int MODE, bool RHO, typename LD>
+__device__ __forceinline__ void dense_apply(LD ld, int blk, C rhob, const cx<C> (&in)[4][3], cx<C> (&out)[4][3])
+{
+#pragma unroll
+  for (int r = 0; r < 6; r++) {
+    C re1 = 0, im1 = 0, re2 = 0, im2 = 0;
+#pragma unroll
+    for (int c = 0; c < 6; c++) {
+      const cx<C> a = ld(r, c);
+      const cx<C> w = in[2 * blk + c / 3][c % 3];
+      if (c < 3) {
+        re1 = fma(a.re, w.re, re1);
+        re1 = fma(-a.im, w.im, re1);
+        im1 = fma(a.re, w.im, im1);
+        im1 = fma(a.im, w.re, im1);
+      } else {
+        re2 = fma(a.re, w.re, re2);
+        re2 = fma(-a.im, w.im, re2);
+        im2 = fma(a.re, w.im, im2);
+        im2 = fma(a.im, w.re, im2);
+      }
+    }
+    C re = re1 + re2, im = im1 + im2;
+    if (RHO) {
+      const cx<C> v = in[2 * blk + r / 3][r % 3];
+      re = fma(-rhob, v.im, re);
+      im = fma(rhob, v.re, im);
+    }
+    cx<C> &o = out[2 * blk + r / 3][r % 3];
+    if (MODE == MODE_ADD) {
+      o.re = o.re + re;
+      o.im = o.im + im;
+    } else {
+      o.re = re;
+      o.im = im;
+    }
+  }
+}
+
+// the rho of block blk with its sign: + i rho g5 for plus, - for minus
+template <typename C> __device__ __forceinline__ C rho_of_block(int blk, int isPlus, C rho)
+{
+  return ((isPlus != 0) != (blk == 1)) ? rho : -rho;
+}
+
+// out (MODE) A in, A the Hermitian CloverBlock block `blk` read from global
+// memory; base = tile*72*V + lane
+template <typename FT, int MODE, bool RHO>
 __device__ __forceinline__ void clover_block(const elem_t<FT> *__restrict__ cl, long long base, int V, int blk,
+                                             typename ftraits<FT>::C rhob,
                                              const cx<typename ftraits<FT>::C> (&in)[4][3],
-                                             cx<typename ftraits<FT>::C> (&res)[4][3])
+                                             cx<typename ftraits<FT>::C> (&out)[4][3])
 {
   typedef typename ftraits<FT>::C C;
   const elem_t<FT> *p = cl + base + (long long)blk * 36 * V;
@@ -455,70 +563,25 @@ __device__ __forceinline__ void clover_block(const elem_t<FT> *__restrict__ cl, 
     od[i].re = ftraits<FT>::ld(p + (long long)(6 + 2 * i) * V);
     od[i].im = ftraits<FT>::ld(p + (long long)(7 + 2 * i) * V);
   }
-#pragma unroll
-  for (int r = 0; r < 6; r++) {
-    const cx<C> v = in[2 * blk + r / 3][r % 3];
-    C re = dg[r] * v.re, im = dg[r] * v.im;
-#pragma unroll
-    for (int c = 0; c < 6; c++) {
-      if (c == r) continue;
-      const cx<C> w = in[2 * blk + c / 3][c % 3];
-      if (r > c) { // A[r][c] = od[r(r-1)/2+c]
-        const cx<C> a = od[r * (r - 1) / 2 + c];
-        re = fma(a.re, w.re, re);
-        re = fma(-a.im, w.im, re);
-        im = fma(a.re, w.im, im);
-        im = fma(a.im, w.re, im);
-      } else { // A[r][c] = conj(od[c(c-1)/2+r])
-        const cx<C> a = od[c * (c - 1) / 2 + r];
-        re = fma(a.re, w.re, re);
-        re = fma(a.im, w.im, re);
-        im = fma(a.re, w.im, im);
-        im = fma(-a.im, w.re, im);
-      }
-    }
-    cx<C> &o = res[2 * blk + r / 3][r % 3];
-    if (ACC) {
-      o.re += re;
-      o.im += im;
-    } else {
-      o.re = re;
-      o.im = im;
-    }
-  }
+  herm_apply<C, MODE, RHO>(dg, od, blk, rhob, in, out);
 }
 
-// res (+)= F in, F a dense FullCloverBlock block (dslash_common.cc:1188-1232).
-// base = tile*144*V + lane.
-template <typename FT, bool ACC>
+// out (MODE) F in, F a dense FullCloverBlock block read from global memory;
+// base = tile*144*V + lane
+template <typename FT, int MODE, bool RHO>
 __device__ __forceinline__ void full_clover_block(const elem_t<FT> *__restrict__ cl, long long base, int V, int blk,
+                                                  typename ftraits<FT>::C rhob,
                                                   const cx<typename ftraits<FT>::C> (&in)[4][3],
-                                                  cx<typename ftraits<FT>::C> (&res)[4][3])
+                                                  cx<typename ftraits<FT>::C> (&out)[4][3])
 {
   typedef typename ftraits<FT>::C C;
   const elem_t<FT> *p = cl + base + (long long)blk * 72 * V;
-#pragma unroll
-  for (int r = 0; r < 6; r++) {
-    C re = 0, im = 0;
-#pragma unroll
-    for (int c = 0; c < 6; c++) {
-      const C ar = ftraits<FT>::ld(p + (long long)((r * 6 + c) * 2 + 0) * V);
-      const C ai = ftraits<FT>::ld(p + (long long)((r * 6 + c) * 2 + 1) * V);
-      const cx<C> w = in[2 * blk + c / 3][c % 3];
-      re = fma(ar, w.re, re);
-      re = fma(-ai, w.im, re);
-      im = fma(ar, w.im, im);
-      im = fma(ai, w.re, im);
-    }
-    cx<C> &o = res[2 * blk + r / 3][r % 3];
-    if (ACC) {
-      o.re += re;
-      o.im += im;
-    } else {
-      o.re = re;
-      o.im = im;
-    }
-  }
+  dense_apply<C, MODE, RHO>(
+      [&](int r, int c) {
+        return mk<C>(ftraits<FT>::ld(p + (long long)((r * 6 + c) * 2 + 0) * V),
+                     ftraits<FT>::ld(p + (long long)((r * 6 + c) * 2 + 1) * V));
+      },
+      blk, rhob, in, out);
 }
 
 // res (+)= muinv (1 + sg i mu) in, sg = -1 on the upper spins for plus

@@ -170,8 +170,8 @@ __device__ __forceinline__ void unpack_one(const elem_t<FT> *__restrict__ buf,
       const long long cbase = tile * ((FAM == FAM_CLOVER ? 72LL : 144LL) * g.V) + lane;
 #pragma unroll
       for (int blk = 0; blk < 2; blk++) {
-        if (FAM == FAM_CLOVER) clover_block<FT, true>(clov, cbase, g.V, blk, dout, o);
-        else full_clover_block<FT, true>(clov, cbase, g.V, blk, dout, o);
+        if (FAM == FAM_CLOVER) clover_block<FT, MODE_ADD, false>(clov, cbase, g.V, blk, (C)0, dout, o);
+        else full_clover_block<FT, MODE_ADD, false>(clov, cbase, g.V, blk, (C)0, dout, o);
       }
     } else {
       inv_twisted<C, true>(dout, p.isPlus, p.mu, p.muinv, o);

@@ -1,28 +1,25 @@
 // qb200_inst.cu -- kernel instantiations and launchers for one storage type
 // and SOALEN.  Compiled once per (QB_FT, QB_S) pair by the build so that the
 // translation units build in parallel.
+#include <atomic>
 #include <cstdint>
 #include <type_traits>
 
 #include "qb200_face_kernel.cuh"
 #include "qb200_internal.h"
 #include "qb200_staged_kernel.cuh"
-#include "qb200_site2_kernel.cuh"
 #include "qb200_async_kernel.cuh"
+#include "qb200_twin_kernel.cuh"
 
 // the single-RHS operator with the next hop's copies in flight (cp.async)
 #ifndef QB_ASYNC
 #define QB_ASYNC 1
 #endif
+// 16-bit storage: two sites per thread, bulk-copy staging (qb200_twin_kernel.cuh)
+#ifndef QB_TWIN
+#define QB_TWIN 1
+#endif
 
-// two sites per thread (qb200_site2_kernel.cuh) for the single-RHS operator
-#ifndef QB_SITE2
-#define QB_SITE2 0
-#endif
-// prefer it to the staged kernel on narrow layouts
-#ifndef QB_SITE2_OVER_STAGED
-#define QB_SITE2_OVER_STAGED 0
-#endif
 #if QB_MRHS
 #include "qb200_pair_kernel.cuh"
 #endif
@@ -39,6 +36,32 @@ namespace qb200 {
 namespace {
 constexpr int kThreads = 128;
 
+// two sites per thread for 16-bit storage: one warp per 64 sites of a plane
+template <typename FT, int S, bool COMP12, int FAM, bool ACH>
+cudaError_t go_twin(const KArgs<FT> &a, const GeoDev &g, const OpDev<float> &p, cudaStream_t st)
+{
+  typedef TwinCfg<FT, S, COMP12> T;
+  const int nchunk = (g.nxh * g.ny + 63) / 64;
+  const long long nw = (long long)g.nz * g.nt * nchunk;
+  const long long blocks = (nw + kTwinWarps - 1) / kTwinWarps;
+  if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+  const int smem = kTwinWarps * T::WB;
+  // the dynamic shared-memory limit of this kernel, raised once per device
+  static std::atomic<unsigned long long> raised{0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!(raised.load() & (1ull << dev))) {
+    e = cudaFuncSetAttribute(twin_site_kernel<FT, S, COMP12, FAM, ACH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             smem);
+    if (e != cudaSuccess) return e;
+    raised.fetch_or(1ull << dev);
+  }
+  twin_site_kernel<FT, S, COMP12, FAM, ACH><<<(unsigned)blocks, kTwinWarps * 32, smem, st>>>(a, g, p, nchunk);
+  return cudaGetLastError();
+}
+
 template <typename FT, int S, bool COMP12, int FAM, bool ACH, bool MR>
 cudaError_t go(const KArgs<FT> &a, const GeoDev &g, const OpDev<typename ftraits<FT>::C> &p,
                cudaStream_t st)
@@ -47,24 +70,16 @@ cudaError_t go(const KArgs<FT> &a, const GeoDev &g, const OpDev<typename ftraits
   const long long n = (long long)g.nxh * g.ny * (MR ? g.nrhs : 1);
   const dim3 grid((unsigned)((n + kThreads - 1) / kThreads), (unsigned)(g.nz * g.nt));
   if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
+  if constexpr (QB_TWIN && !MR && twin_layout<FT, S>()) {
+    const bool al = (((uintptr_t)a.psi | (uintptr_t)a.out | (uintptr_t)a.gauge) % 16 == 0) &&
+                    (!ACH || (uintptr_t)a.chi % 16 == 0) && ((FAM != FAM_CLOVER && FAM != FAM_TMCLOV) || (uintptr_t)a.clov % 16 == 0);
+    if (g.V == S && al) return go_twin<FT, S, COMP12, FAM, ACH>(a, g, p, st);
+  }
   if constexpr (QB_ASYNC && !MR && async_layout<FT, S>()) {
     const bool al = (((uintptr_t)a.psi | (uintptr_t)a.out | (uintptr_t)a.gauge) % 16 == 0) &&
                     (!ACH || (uintptr_t)a.chi % 16 == 0) && ((FAM != FAM_CLOVER && FAM != FAM_TMCLOV) || (uintptr_t)a.clov % 16 == 0);
     if (g.V == S && al) {
       async_site_kernel<FT, S, COMP12, FAM, ACH><<<grid, kThreads, 0, st>>>(a, g, p);
-      return cudaGetLastError();
-    }
-  }
-  // two sites per thread in packed FP32x2 arithmetic
-  if constexpr (QB_SITE2 && !MR && S >= 2 && !std::is_same<FT, double>::value &&
-                (QB_SITE2_OVER_STAGED || !staged_layout<FT, S>())) {
-    const bool al = (((uintptr_t)a.psi | (uintptr_t)a.out | (uintptr_t)a.gauge) % 8 == 0) &&
-                    (!ACH || (uintptr_t)a.chi % 8 == 0) && (FAM == FAM_WILSON || FAM == FAM_TM ||
-                                                              (uintptr_t)a.clov % 8 == 0);
-    if (al && (p.acc_mask & 3u) == 3u) {
-      const dim3 g2((unsigned)(((long long)(g.nxh / 2) * g.ny + kThreads - 1) / kThreads), (unsigned)(g.nz * g.nt));
-      if (S >= 4 && g.V == S) site2_dslash_kernel<FT, S, COMP12, FAM, ACH, (S >= 4 ? S : 0)><<<g2, kThreads, 0, st>>>(a, g, p);
-      else site2_dslash_kernel<FT, S, COMP12, FAM, ACH, 0><<<g2, kThreads, 0, st>>>(a, g, p);
       return cudaGetLastError();
     }
   }

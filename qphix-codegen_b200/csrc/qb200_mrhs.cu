@@ -594,7 +594,12 @@ int mr_reliable(const qb200_lattice *lat_hi, const qb200_operator *op_hi, const 
     if (!first) {
       // continue the recurrence in the new units: p = r + beta p
       VecScalar beta = vhost(0.0);
-      for (int i = 0; i < nrhs; i++) beta.host[i] = h[i] / (rr[i] * ratio.host[i] * ratio.host[i]);
+      // a right-hand side whose residual is exactly zero (a zero source, or
+      // one already solved exactly) keeps a zero direction instead of 0/0
+      for (int i = 0; i < nrhs; i++) {
+        const double den = rr[i] * ratio.host[i] * ratio.host[i];
+        beta.host[i] = den > 0 ? h[i] / den : 0.0;
+      }
       if ((rc = cuda_rc(mr_axpby(m, vhost(1.0), rl, beta, p, st), "multi-RHS reliable direction"))) return rc;
     }
     for (int i = 0; i < nrhs; i++) {

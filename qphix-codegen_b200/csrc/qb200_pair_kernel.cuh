@@ -170,11 +170,58 @@ __device__ __forceinline__ void recons2(const c2 (&ub)[2][3], float beta, float 
   }
 }
 
-// res[block rows] = A in, A the Hermitian CloverBlock block `blk`
+__device__ __forceinline__ float2 f2add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+
+// herm_apply (qb200_device.cuh) for a pair of right-hand sides: the same
+// chains, operation for operation
+template <int MODE, bool RHO>
+__device__ __forceinline__ void herm_apply2(const float (&dg)[6], const cx<float> (&od)[15], int blk, float rhob,
+                                            const c2 (&in)[4][3], c2 (&out)[4][3])
+{
+#pragma unroll
+  for (int r = 0; r < 6; r++) {
+    const c2 v = in[2 * blk + r / 3][r % 3];
+    float2 re1 = f2mul(bc(dg[r]), v.re), im1 = f2mul(bc(dg[r]), v.im);
+    float2 re2 = bc(0.f), im2 = bc(0.f);
+#pragma unroll
+    for (int c = 0; c < 6; c++) {
+      if (c == r) continue;
+      const c2 w = in[2 * blk + c / 3][c % 3];
+      if (c < r) { // A[r][c] = od[r(r-1)/2+c]
+        const cx<float> a = od[r * (r - 1) / 2 + c];
+        re1 = f2fma(bc(a.re), w.re, re1);
+        re1 = f2fma(bc(-a.im), w.im, re1);
+        im1 = f2fma(bc(a.re), w.im, im1);
+        im1 = f2fma(bc(a.im), w.re, im1);
+      } else { // A[r][c] = conj(od[c(c-1)/2+r])
+        const cx<float> a = od[c * (c - 1) / 2 + r];
+        re2 = f2fma(bc(a.re), w.re, re2);
+        re2 = f2fma(bc(a.im), w.im, re2);
+        im2 = f2fma(bc(a.re), w.im, im2);
+        im2 = f2fma(bc(-a.im), w.re, im2);
+      }
+    }
+    float2 re = f2add(re1, re2), im = f2add(im1, im2);
+    if (RHO) {
+      re = f2fma(bc(-rhob), v.im, re);
+      im = f2fma(bc(rhob), v.re, im);
+    }
+    c2 &o = out[2 * blk + r / 3][r % 3];
+    if (MODE == MODE_ADD) {
+      o.re = f2add(o.re, re);
+      o.im = f2add(o.im, im);
+    } else {
+      o.re = re;
+      o.im = im;
+    }
+  }
+}
+
+// out (MODE) A in, A the Hermitian CloverBlock block `blk`
 // (dslash_common.cc:1098-1186); base = tile*72*V + lane
-template <typename FT>
-__device__ __forceinline__ void clover2(const FT *__restrict__ cl, long long base, int V, int blk,
-                                        const c2 (&in)[4][3], c2 (&res)[4][3])
+template <typename FT, int MODE, bool RHO>
+__device__ __forceinline__ void clover2(const FT *__restrict__ cl, long long base, int V, int blk, float rhob,
+                                        const c2 (&in)[4][3], c2 (&out)[4][3])
 {
   const FT *p = cl + base + (long long)blk * 36 * V;
   float dg[6];
@@ -186,49 +233,50 @@ __device__ __forceinline__ void clover2(const FT *__restrict__ cl, long long bas
     od[i].re = ftraits<FT>::ld(p + (long long)(6 + 2 * i) * V);
     od[i].im = ftraits<FT>::ld(p + (long long)(7 + 2 * i) * V);
   }
-#pragma unroll
-  for (int r = 0; r < 6; r++) {
-    const c2 v = in[2 * blk + r / 3][r % 3];
-    float2 re = f2mul(bc(dg[r]), v.re), im = f2mul(bc(dg[r]), v.im);
-#pragma unroll
-    for (int c = 0; c < 6; c++) {
-      if (c == r) continue;
-      const c2 w = in[2 * blk + c / 3][c % 3];
-      // A[r][c] = od[r(r-1)/2+c] below the diagonal, conj(od[c(c-1)/2+r]) above
-      const cx<float> a = r > c ? od[r * (r - 1) / 2 + c] : od[c * (c - 1) / 2 + r];
-      const float ai = r > c ? a.im : -a.im;
-      re = f2fma(bc(a.re), w.re, re);
-      re = f2fma(bc(-ai), w.im, re);
-      im = f2fma(bc(a.re), w.im, im);
-      im = f2fma(bc(ai), w.re, im);
-    }
-    res[2 * blk + r / 3][r % 3].re = re;
-    res[2 * blk + r / 3][r % 3].im = im;
-  }
+  herm_apply2<MODE, RHO>(dg, od, blk, rhob, in, out);
 }
 
-// res[block rows] = F in, F a dense FullCloverBlock block
-// (dslash_common.cc:1188-1232); base = tile*144*V + lane
-template <typename FT>
-__device__ __forceinline__ void full_clover2(const FT *__restrict__ cl, long long base, int V, int blk,
-                                             const c2 (&in)[4][3], c2 (&res)[4][3])
+// out (MODE) F in, F a dense FullCloverBlock block (dslash_common.cc:1188-1232),
+// dense_apply's chains; base = tile*144*V + lane
+template <typename FT, int MODE, bool RHO>
+__device__ __forceinline__ void full_clover2(const FT *__restrict__ cl, long long base, int V, int blk, float rhob,
+                                             const c2 (&in)[4][3], c2 (&out)[4][3])
 {
   const FT *p = cl + base + (long long)blk * 72 * V;
 #pragma unroll
   for (int r = 0; r < 6; r++) {
-    float2 re = bc(0.f), im = bc(0.f);
+    float2 re1 = bc(0.f), im1 = bc(0.f), re2 = bc(0.f), im2 = bc(0.f);
 #pragma unroll
     for (int c = 0; c < 6; c++) {
       const float ar = ftraits<FT>::ld(p + (long long)((r * 6 + c) * 2 + 0) * V);
       const float ai = ftraits<FT>::ld(p + (long long)((r * 6 + c) * 2 + 1) * V);
       const c2 w = in[2 * blk + c / 3][c % 3];
-      re = f2fma(bc(ar), w.re, re);
-      re = f2fma(bc(-ai), w.im, re);
-      im = f2fma(bc(ar), w.im, im);
-      im = f2fma(bc(ai), w.re, im);
+      if (c < 3) {
+        re1 = f2fma(bc(ar), w.re, re1);
+        re1 = f2fma(bc(-ai), w.im, re1);
+        im1 = f2fma(bc(ar), w.im, im1);
+        im1 = f2fma(bc(ai), w.re, im1);
+      } else {
+        re2 = f2fma(bc(ar), w.re, re2);
+        re2 = f2fma(bc(-ai), w.im, re2);
+        im2 = f2fma(bc(ar), w.im, im2);
+        im2 = f2fma(bc(ai), w.re, im2);
+      }
     }
-    res[2 * blk + r / 3][r % 3].re = re;
-    res[2 * blk + r / 3][r % 3].im = im;
+    float2 re = f2add(re1, re2), im = f2add(im1, im2);
+    if (RHO) {
+      const c2 v = in[2 * blk + r / 3][r % 3];
+      re = f2fma(bc(-rhob), v.im, re);
+      im = f2fma(bc(rhob), v.re, im);
+    }
+    c2 &o = out[2 * blk + r / 3][r % 3];
+    if (MODE == MODE_ADD) {
+      o.re = f2add(o.re, re);
+      o.im = f2add(o.im, im);
+    } else {
+      o.re = re;
+      o.im = im;
+    }
   }
 }
 
@@ -302,8 +350,15 @@ __global__ void __launch_bounds__(128, (ACH && FAM != FAM_TMCLOV) ? QB_PAIR_MINB
   const int le = nr;
   const int cs = S * nr;
 
-  c2 res[4][3];
+  c2 acc[4][3], res[4][3];
+#pragma unroll
+  for (int sp2 = 0; sp2 < 4; sp2++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) acc[sp2][c].re = acc[sp2][c].im = bc(0.f);
+  hops2<FT, S, COMP12, VV>(a, g, p, s, obase, ue, le, cs, gbase, acc);
   if (ACH) {
+    // the hops (subtracted: beta arrives negated from the host), then + A.chi
+    // (ach_finish's operations)
     c2 ch[4][3];
     load_pair<FT>(a.chi, obase, cs, ch);
     if (FAM == FAM_WILSON) {
@@ -311,8 +366,8 @@ __global__ void __launch_bounds__(128, (ACH && FAM != FAM_TMCLOV) ? QB_PAIR_MINB
       for (int sp2 = 0; sp2 < 4; sp2++)
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-          res[sp2][c].re = f2mul(bc(p.alpha), ch[sp2][c].re);
-          res[sp2][c].im = f2mul(bc(p.alpha), ch[sp2][c].im);
+          acc[sp2][c].re = f2fma(bc(p.alpha), ch[sp2][c].re, acc[sp2][c].re);
+          acc[sp2][c].im = f2fma(bc(p.alpha), ch[sp2][c].im, acc[sp2][c].im);
         }
     } else if (FAM == FAM_TM) {
       // alpha (1 +/- i mu g5) chi, + on the upper spins for plus
@@ -321,43 +376,30 @@ __global__ void __launch_bounds__(128, (ACH && FAM != FAM_TMCLOV) ? QB_PAIR_MINB
         const float m = (((sp2 < 2) == (p.isPlus != 0)) ? 1.f : -1.f) * p.mu;
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-          res[sp2][c].re = f2mul(bc(p.alpha), f2fma(bc(-m), ch[sp2][c].im, ch[sp2][c].re));
-          res[sp2][c].im = f2mul(bc(p.alpha), f2fma(bc(m), ch[sp2][c].re, ch[sp2][c].im));
+          acc[sp2][c].re = f2fma(bc(p.alpha), f2fma(bc(-m), ch[sp2][c].im, ch[sp2][c].re), acc[sp2][c].re);
+          acc[sp2][c].im = f2fma(bc(p.alpha), f2fma(bc(m), ch[sp2][c].re, ch[sp2][c].im), acc[sp2][c].im);
         }
       }
     } else {
       const long long cbase = tile * ((FAM == FAM_CLOVER ? 72LL : 144LL) * V) + lane;
 #pragma unroll
       for (int blk = 0; blk < 2; blk++) {
-        if (FAM == FAM_CLOVER) clover2<FT>(a.clov, cbase, V, blk, ch, res);
-        else full_clover2<FT>(a.clov, cbase, V, blk, ch, res);
-      }
-      // + i rho g5 chi for plus (dslash_common.cc:1873-1906)
-#pragma unroll
-      for (int sp2 = 0; sp2 < 4; sp2++) {
-        const float r = (((p.isPlus != 0) != (sp2 >= 2)) ? 1.f : -1.f) * p.rho;
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-          res[sp2][c].re = f2fma(bc(-r), ch[sp2][c].im, res[sp2][c].re);
-          res[sp2][c].im = f2fma(bc(r), ch[sp2][c].re, res[sp2][c].im);
-        }
+        const float rb = rho_of_block<float>(blk, p.isPlus, p.rho);
+        if (FAM == FAM_CLOVER) clover2<FT, MODE_ADD, true>(a.clov, cbase, V, blk, rb, ch, acc);
+        else full_clover2<FT, MODE_ADD, true>(a.clov, cbase, V, blk, rb, ch, acc);
       }
     }
-    // the hops are subtracted: beta arrives negated from the host
-    hops2<FT, S, COMP12, VV>(a, g, p, s, obase, ue, le, cs, gbase, res);
-  } else {
-    c2 acc[4][3];
 #pragma unroll
     for (int sp2 = 0; sp2 < 4; sp2++)
 #pragma unroll
-      for (int c = 0; c < 3; c++) acc[sp2][c].re = acc[sp2][c].im = bc(0.f);
-    hops2<FT, S, COMP12, VV>(a, g, p, s, obase, ue, le, cs, gbase, acc);
+      for (int c = 0; c < 3; c++) res[sp2][c] = acc[sp2][c];
+  } else {
     if (FAM == FAM_CLOVER || FAM == FAM_TMCLOV) {
       const long long cbase = tile * ((FAM == FAM_CLOVER ? 72LL : 144LL) * V) + lane;
 #pragma unroll
       for (int blk = 0; blk < 2; blk++) {
-        if (FAM == FAM_CLOVER) clover2<FT>(a.clov, cbase, V, blk, acc, res);
-        else full_clover2<FT>(a.clov, cbase, V, blk, acc, res);
+        if (FAM == FAM_CLOVER) clover2<FT, MODE_SET, false>(a.clov, cbase, V, blk, 0.f, acc, res);
+        else full_clover2<FT, MODE_SET, false>(a.clov, cbase, V, blk, 0.f, acc, res);
       }
     } else if (FAM == FAM_TM) {
       // muinv (1 + sg i mu) acc, sg = -1 on the upper spins for plus

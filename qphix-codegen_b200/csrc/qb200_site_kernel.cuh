@@ -98,44 +98,43 @@ __device__ __forceinline__ void do_hop(const KArgs<FT> &a, const GeoDev &g,
   recons<C, MU>(ub, beta, tau, acc);
 }
 
-// A.chi + (i rho g5 chi) into res: the pre-term of the achimbdpsi form
-// (achiResult, dslash_common.cc:1559-1655; rho term :1873-1906)
+// acc += A.chi (+ i rho g5 chi): the A.chi term of the achimbdpsi form
+// (achiResult, dslash_common.cc:1559-1655; rho term :1873-1906), added to
+// the hops already summed in acc (beta negated by the host), one rounding
+// per component after the term itself.  Wilson: A = alpha; twisted mass:
+// alpha (1 +/- i mu g5), + on the upper spins for plus.
 template <typename FT, int FAM>
-__device__ __forceinline__ void ach_pre(const KArgs<FT> &a, const OpDev<typename ftraits<FT>::C> &p, long long tile,
-                                        int lane, int V, const cx<typename ftraits<FT>::C> (&ch)[4][3],
-                                        cx<typename ftraits<FT>::C> (&res)[4][3])
+__device__ __forceinline__ void ach_finish(const KArgs<FT> &a, const OpDev<typename ftraits<FT>::C> &p,
+                                           long long tile, int lane, int V,
+                                           const cx<typename ftraits<FT>::C> (&ch)[4][3],
+                                           cx<typename ftraits<FT>::C> (&acc)[4][3])
 {
   typedef typename ftraits<FT>::C C;
   if (FAM == FAM_WILSON) {
 #pragma unroll
     for (int sp = 0; sp < 4; sp++)
 #pragma unroll
-      for (int c = 0; c < 3; c++) res[sp][c] = mk<C>(p.alpha * ch[sp][c].re, p.alpha * ch[sp][c].im);
+      for (int c = 0; c < 3; c++) {
+        acc[sp][c].re = fma(p.alpha, ch[sp][c].re, acc[sp][c].re);
+        acc[sp][c].im = fma(p.alpha, ch[sp][c].im, acc[sp][c].im);
+      }
   } else if (FAM == FAM_TM) {
-    // alpha (1 +/- i mu g5) chi, + on the upper spins for plus
 #pragma unroll
     for (int sp = 0; sp < 4; sp++) {
       const C m = (((sp < 2) == (p.isPlus != 0)) ? (C)1 : (C)-1) * p.mu;
 #pragma unroll
-      for (int c = 0; c < 3; c++)
-        res[sp][c] = mk<C>(p.alpha * fma(-m, ch[sp][c].im, ch[sp][c].re),
-                           p.alpha * fma(m, ch[sp][c].re, ch[sp][c].im));
+      for (int c = 0; c < 3; c++) {
+        acc[sp][c].re = fma(p.alpha, fma(-m, ch[sp][c].im, ch[sp][c].re), acc[sp][c].re);
+        acc[sp][c].im = fma(p.alpha, fma(m, ch[sp][c].re, ch[sp][c].im), acc[sp][c].im);
+      }
     }
   } else {
     const long long cbase = tile * ((FAM == FAM_CLOVER ? 72LL : 144LL) * V) + lane;
 #pragma unroll
     for (int blk = 0; blk < 2; blk++) {
-      if (FAM == FAM_CLOVER) clover_block<FT, false>(a.clov, cbase, V, blk, ch, res);
-      else full_clover_block<FT, false>(a.clov, cbase, V, blk, ch, res);
-    }
-#pragma unroll
-    for (int sp = 0; sp < 4; sp++) {
-      const C r = (((p.isPlus != 0) != (sp >= 2)) ? (C)1 : (C)-1) * p.rho;
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        res[sp][c].re = fma(-r, ch[sp][c].im, res[sp][c].re);
-        res[sp][c].im = fma(r, ch[sp][c].re, res[sp][c].im);
-      }
+      const C rb = rho_of_block<C>(blk, p.isPlus, p.rho);
+      if (FAM == FAM_CLOVER) clover_block<FT, MODE_ADD, true>(a.clov, cbase, V, blk, rb, ch, acc);
+      else full_clover_block<FT, MODE_ADD, true>(a.clov, cbase, V, blk, rb, ch, acc);
     }
   }
 }
@@ -153,8 +152,8 @@ __device__ __forceinline__ void plain_post(const KArgs<FT> &a, const OpDev<typen
     const long long cbase = tile * ((FAM == FAM_CLOVER ? 72LL : 144LL) * V) + lane;
 #pragma unroll
     for (int blk = 0; blk < 2; blk++) {
-      if (FAM == FAM_CLOVER) clover_block<FT, false>(a.clov, cbase, V, blk, acc, res);
-      else full_clover_block<FT, false>(a.clov, cbase, V, blk, acc, res);
+      if (FAM == FAM_CLOVER) clover_block<FT, MODE_SET, false>(a.clov, cbase, V, blk, (C)0, acc, res);
+      else full_clover_block<FT, MODE_SET, false>(a.clov, cbase, V, blk, (C)0, acc, res);
     }
   } else if (FAM == FAM_TM) {
     inv_twisted<C, false>(acc, p.isPlus, p.mu, p.muinv, res);
@@ -199,26 +198,23 @@ __device__ __forceinline__ void site_body(const KArgs<FT> &a, const GeoDev &g,
   const int le = nr;
   const int cs = S * nr;
 
-  cx<C> res[4][3];
+  cx<C> res[4][3], acc[4][3];
 #pragma unroll
   for (int sp = 0; sp < 4; sp++)
 #pragma unroll
-    for (int c = 0; c < 3; c++) res[sp][c] = mk<C>(0, 0);
-
+    for (int c = 0; c < 3; c++) acc[sp][c] = mk<C>(0, 0);
+  all_hops<FT, S, COMP12, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
   if (ACH) {
-    // A.chi first, then the hops are subtracted (beta already negated by the host)
+    // the hops (subtracted: beta negated by the host), then + A.chi
     cx<C> ch[4][3];
     if (MR) load_spinor_rs<FT>(a.chi, obase, cs, ch);
     else load_spinor<FT, S>(a.chi, obase, ch);
-    ach_pre<FT, FAM>(a, p, tile, lane, V, ch, res);
-    all_hops<FT, S, COMP12, MR, VV>(a, g, p, s, obase, ue, le, gbase, res);
-  } else {
-    cx<C> acc[4][3];
+    ach_finish<FT, FAM>(a, p, tile, lane, V, ch, acc);
 #pragma unroll
     for (int sp = 0; sp < 4; sp++)
 #pragma unroll
-      for (int c = 0; c < 3; c++) acc[sp][c] = mk<C>(0, 0);
-    all_hops<FT, S, COMP12, MR, VV>(a, g, p, s, obase, ue, le, gbase, acc);
+      for (int c = 0; c < 3; c++) res[sp][c] = acc[sp][c];
+  } else {
     plain_post<FT, FAM>(a, p, tile, lane, V, acc, res);
   }
   if (MR) store_spinor_rs<FT>(a.out, obase, cs, res);

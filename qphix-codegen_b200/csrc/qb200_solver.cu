@@ -673,7 +673,10 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[QB200_NOALLOC_S
 
 namespace {
 // device address of g_noalloc_scratch, looked up once per device (with that
-// device current) by the first call made on it
+// device current) by the first call made on it.  The address is kept for the
+// life of the process: after cudaDeviceReset (or any teardown of the
+// device's primary context) it would name freed memory, so the entry point
+// must not be used across a device reset.
 void *noalloc_scratch(int *rc)
 {
   static std::mutex mu;

@@ -185,9 +185,9 @@ __device__ __forceinline__ void load_link_sm(const unsigned char *grp, int lane,
 }
 
 // clover_block from a staged CloverBlock half (the same operations)
-template <typename FT, int S>
-__device__ __forceinline__ void clover_block_sm(const unsigned char *grp, int lane, int blk,
-                                                const cx<comp_t<FT>> (&in)[4][3], cx<comp_t<FT>> (&res)[4][3])
+template <typename FT, int S, int MODE, bool RHO>
+__device__ __forceinline__ void clover_block_sm(const unsigned char *grp, int lane, int blk, comp_t<FT> rhob,
+                                                const cx<comp_t<FT>> (&in)[4][3], cx<comp_t<FT>> (&out)[4][3])
 {
   typedef comp_t<FT> C;
   C dg[6];
@@ -199,31 +199,7 @@ __device__ __forceinline__ void clover_block_sm(const unsigned char *grp, int la
     od[i].re = sm_ld<FT, S>(grp, 6 + 2 * i, lane);
     od[i].im = sm_ld<FT, S>(grp, 7 + 2 * i, lane);
   }
-#pragma unroll
-  for (int r = 0; r < 6; r++) {
-    const cx<C> v = in[2 * blk + r / 3][r % 3];
-    C re = dg[r] * v.re, im = dg[r] * v.im;
-#pragma unroll
-    for (int c = 0; c < 6; c++) {
-      if (c == r) continue;
-      const cx<C> w = in[2 * blk + c / 3][c % 3];
-      if (r > c) {
-        const cx<C> a = od[r * (r - 1) / 2 + c];
-        re = fma(a.re, w.re, re);
-        re = fma(-a.im, w.im, re);
-        im = fma(a.re, w.im, im);
-        im = fma(a.im, w.re, im);
-      } else {
-        const cx<C> a = od[c * (c - 1) / 2 + r];
-        re = fma(a.re, w.re, re);
-        re = fma(a.im, w.im, re);
-        im = fma(a.re, w.im, im);
-        im = fma(-a.im, w.re, im);
-      }
-    }
-    res[2 * blk + r / 3][r % 3].re = re;
-    res[2 * blk + r / 3][r % 3].im = im;
-  }
+  herm_apply<C, MODE, RHO>(dg, od, blk, rhob, in, out);
 }
 
 struct WarpCtx {
@@ -304,10 +280,11 @@ __device__ __forceinline__ void staged_hops(const KArgs<FT> &a, const GeoDev &g,
   staged_hop<FT, S, COMP12, 7>(a, g, p, s, obase, w, acc);
 }
 
-// res (+)= the CloverBlock of the site's tile applied to in, both halves staged
-template <typename FT, int S>
-__device__ __forceinline__ void staged_clover(const KArgs<FT> &a, const WarpCtx &w,
-                                              const cx<comp_t<FT>> (&in)[4][3], cx<comp_t<FT>> (&res)[4][3])
+// out (MODE) the CloverBlock of the site's tile applied to in (RHO: with
+// the + i rho g5 in term), both halves staged
+template <typename FT, int S, int MODE, bool RHO>
+__device__ __forceinline__ void staged_clover(const KArgs<FT> &a, const WarpCtx &w, int isPlus, comp_t<FT> rho,
+                                              const cx<comp_t<FT>> (&in)[4][3], cx<comp_t<FT>> (&out)[4][3])
 {
   typedef Stage<FT, S> St;
   constexpr int CLB = 36 * S * (int)sizeof(elem_t<FT>);
@@ -315,17 +292,18 @@ __device__ __forceinline__ void staged_clover(const KArgs<FT> &a, const WarpCtx 
   for (int blk = 0; blk < 2; blk++) {
     stage_in<FT, S, CLB, St::CL>(a.clov, w.tile * (72LL * S) + blk * 36LL * S, w.buf, w.ln);
     __syncwarp();
-    clover_block_sm<FT, S>(w.buf + (w.ln / S) * St::CL, w.lane, blk, in, res);
+    clover_block_sm<FT, S, MODE, RHO>(w.buf + (w.ln / S) * St::CL, w.lane, blk,
+                                      rho_of_block<comp_t<FT>>(blk, isPlus, rho), in, out);
     __syncwarp();
   }
 }
 
-// res = the FullCloverBlock of the site's tile applied to in (dense 6x6
-// complex per half, full_clover_block's operation order), both halves
-// staged; buf needs Stage::G * Stage::stride(72) bytes
-template <typename FT, int S>
-__device__ __forceinline__ void staged_full_clover(const KArgs<FT> &a, const WarpCtx &w,
-                                                   const cx<comp_t<FT>> (&in)[4][3], cx<comp_t<FT>> (&res)[4][3])
+// out (MODE) the FullCloverBlock of the site's tile applied to in (dense 6x6
+// complex per half, dense_apply's operation order; RHO: with the + i rho g5
+// in term), both halves staged; buf needs Stage::G * Stage::stride(72) bytes
+template <typename FT, int S, int MODE, bool RHO>
+__device__ __forceinline__ void staged_full_clover(const KArgs<FT> &a, const WarpCtx &w, int isPlus, comp_t<FT> rho,
+                                                   const cx<comp_t<FT>> (&in)[4][3], cx<comp_t<FT>> (&out)[4][3])
 {
   typedef comp_t<FT> C;
   typedef Stage<FT, S> St;
@@ -336,21 +314,12 @@ __device__ __forceinline__ void staged_full_clover(const KArgs<FT> &a, const War
     stage_in<FT, S, FCB, FCS>(a.clov, w.tile * (144LL * S) + blk * 72LL * S, w.buf, w.ln);
     __syncwarp();
     const unsigned char *grp = w.buf + (w.ln / S) * FCS;
-#pragma unroll
-    for (int r = 0; r < 6; r++) {
-      C re = 0, im = 0;
-#pragma unroll
-      for (int c = 0; c < 6; c++) {
-        const C ar = sm_ld<FT, S>(grp, (r * 6 + c) * 2 + 0, w.lane);
-        const C ai = sm_ld<FT, S>(grp, (r * 6 + c) * 2 + 1, w.lane);
-        const cx<C> v = in[2 * blk + c / 3][c % 3];
-        re = fma(ar, v.re, re);
-        re = fma(-ai, v.im, re);
-        im = fma(ar, v.im, im);
-        im = fma(ai, v.re, im);
-      }
-      res[2 * blk + r / 3][r % 3] = mk<C>(re, im);
-    }
+    const int lane = w.lane;
+    dense_apply<C, MODE, RHO>(
+        [&](int r, int c) {
+          return mk<C>(sm_ld<FT, S>(grp, (r * 6 + c) * 2 + 0, lane), sm_ld<FT, S>(grp, (r * 6 + c) * 2 + 1, lane));
+        },
+        blk, rho_of_block<C>(blk, isPlus, rho), in, out);
     __syncwarp();
   }
 }
@@ -386,44 +355,32 @@ __device__ __forceinline__ void staged_body(const KArgs<FT> &a, const GeoDev &g,
   w.blk0 = __shfl_sync(0xffffffffu, w.blk, 0);
   constexpr int SPB = St::SPB * S * (int)sizeof(elem_t<FT>);
 
-  cx<C> res[4][3];
+  cx<C> acc[4][3];
 #pragma unroll
   for (int sp = 0; sp < 4; sp++)
 #pragma unroll
-    for (int c = 0; c < 3; c++) res[sp][c] = mk<C>(0, 0);
+    for (int c = 0; c < 3; c++) acc[sp][c] = mk<C>(0, 0);
+  staged_hops<FT, S, COMP12>(a, g, p, s, obase, w, acc);
   if (ACH) {
+    // the hops (subtracted: beta negated by the host), then + A.chi
     cx<C> ch[4][3];
     stage_in<FT, S, SPB, St::SP>(a.chi, w.own, w.buf, w.ln);
     __syncwarp();
     load_spinor_sm<FT, S>(w.buf + (w.ln / S) * St::SP, w.lane, ch);
     __syncwarp();
-    if (FAM == FAM_CLOVER) {
-      staged_clover<FT, S>(a, w, ch, res);
-#pragma unroll
-      for (int sp = 0; sp < 4; sp++) {
-        const C r = (((p.isPlus != 0) != (sp >= 2)) ? (C)1 : (C)-1) * p.rho;
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-          res[sp][c].re = fma(-r, ch[sp][c].im, res[sp][c].re);
-          res[sp][c].im = fma(r, ch[sp][c].re, res[sp][c].im);
-        }
-      }
-    } else {
-      ach_pre<FT, FAM>(a, p, w.tile, w.lane, S, ch, res);
-    }
-    staged_hops<FT, S, COMP12>(a, g, p, s, obase, w, res);
+    if (FAM == FAM_CLOVER) staged_clover<FT, S, MODE_ADD, true>(a, w, p.isPlus, p.rho, ch, acc);
+    else ach_finish<FT, FAM>(a, p, w.tile, w.lane, S, ch, acc);
   } else {
-    cx<C> acc[4][3];
+    cx<C> res[4][3];
+    if (FAM == FAM_CLOVER) staged_clover<FT, S, MODE_SET, false>(a, w, p.isPlus, (C)0, acc, res);
+    else plain_post<FT, FAM>(a, p, w.tile, w.lane, S, acc, res);
 #pragma unroll
     for (int sp = 0; sp < 4; sp++)
 #pragma unroll
-      for (int c = 0; c < 3; c++) acc[sp][c] = mk<C>(0, 0);
-    staged_hops<FT, S, COMP12>(a, g, p, s, obase, w, acc);
-    if (FAM == FAM_CLOVER) staged_clover<FT, S>(a, w, acc, res);
-    else plain_post<FT, FAM>(a, p, w.tile, w.lane, S, acc, res);
+      for (int c = 0; c < 3; c++) acc[sp][c] = res[sp][c];
   }
   // the result through shared memory, out in 16-byte vectors
-  store_spinor_sm<FT, S>(w.buf + (w.ln / S) * St::SP, w.lane, res);
+  store_spinor_sm<FT, S>(w.buf + (w.ln / S) * St::SP, w.lane, acc);
   __syncwarp();
   stage_out<FT, S, SPB, St::SP>(a.out, w.own, w.buf, w.ln, active);
   __syncwarp();

@@ -59,17 +59,62 @@ def make_fields(g: Geometry, seed=1234, cb=0, inverse_clover=False):
     return out
 
 
-def site_rel_err(g: Geometry, a, b):
+# Parity tolerances (per site component, relative, floored at the site's rms
+# component; see site_rel_err), GPU result against the FP64 oracle's
+# unrounded result on the same stored inputs:
+#   FP32 1e-6 and FP64 1e-13 (the accuracy the operator must keep);
+#   FP16 (IEEE binary16, the reference's `half`) and FP16 + per-site norm
+#   1e-3: storing the result rounds each component to 11 significant bits,
+#   at most 2^-11 = 4.9e-4 of max(|component|, site rms);
+#   BF16 4e-3: the format limit.  8 significant bits give a unit roundoff of
+#   2^-8 = 3.9e-3 for the one rounding of the stored result, which no
+#   arithmetic can beat; 1e-3 is out of reach for this format.
+TOL = {F32: 1e-6, F64: 1e-13, F16: 1e-3, F16N: 1e-3, BF16: 4e-3}
+
+# worst error seen per parity check, printed at the end of the session
+PARITY = {}
+
+
+def record(name, err, tol=None):
+    """Keep the worst error of a named parity check (and its bound)."""
+    old = PARITY.get(name)
+    if old is None or err > old[0]:
+        PARITY[name] = (float(err), tol)
+    return err
+
+
+def site_rel_err(g: Geometry, a, b, gb: Geometry = None):
     """max over components of |a-b| / max(|b_i|, |b_site|/sqrt(24)) -- the
-    per-component relative error with a floor at the site's rms component."""
+    per-component relative error with a floor at the site's rms component.
+    a is a spinor array of lattice g, b of lattice gb (default g), so that a
+    16-bit result can be compared with an FP64 one."""
+    gb = gb if gb is not None else g
     ta = layout.unpack_spinor(g, to_torch(np.asarray(a)[: g.spinor_elems])).numpy().reshape(-1, 12)
-    tb = layout.unpack_spinor(g, to_torch(np.asarray(b)[: g.spinor_elems])).numpy().reshape(-1, 12)
+    tb = layout.unpack_spinor(gb, to_torch(np.asarray(b)[: gb.spinor_elems])).numpy().reshape(-1, 12)
     ra = np.concatenate([ta.real, ta.imag], axis=1)
     rb = np.concatenate([tb.real, tb.imag], axis=1)
     site = np.sqrt((rb ** 2).sum(axis=1, keepdims=True) / 24.0)
     den = np.maximum(np.abs(rb), site)
     den = np.where(den == 0, 1.0, den)
     return float((np.abs(ra - rb) / den).max())
+
+
+def as_f64(g: Geometry, a):
+    """A stored spinor array of lattice g as an FP64 array of the same layout
+    (ftype F64): the values exactly as stored, decoded."""
+    t = layout.unpack_spinor(g, to_torch(np.asarray(a)[: g.spinor_elems]))
+    return layout.pack_spinor(g.with_(ftype=F64), t, torch.float64).numpy()
+
+
+def face_rel_err(a, b):
+    """face records (n, 12) as float64: max over components of |a-b| /
+    max(|b_i|, rms of the record)"""
+    a = np.asarray(a, dtype=np.float64).reshape(-1, 12)
+    b = np.asarray(b, dtype=np.float64).reshape(-1, 12)
+    rms = np.sqrt((b ** 2).mean(axis=1, keepdims=True))
+    den = np.maximum(np.abs(b), rms)
+    den = np.where(den == 0, 1.0, den)
+    return float((np.abs(a - b) / den).max()) if a.size else 0.0
 
 
 def op_params(family, kernel, seed=0, tbc_mask=0, accumulate=None, coeff=None):

@@ -1,6 +1,7 @@
-"""GPU face kernels against the oracle, and the t-slab decomposition (body
-without slab-crossing hops + face pack/exchange/unpack) emulated on one GPU
-against the full-lattice kernel."""
+"""GPU face kernels against the FP64 oracle (unrounded results, tolerances
+helpers.TOL), and the t-slab decomposition (body without slab-crossing hops +
+face pack/exchange/unpack) emulated on one GPU against the full-lattice
+kernel."""
 import numpy as np
 import pytest
 import torch
@@ -9,10 +10,10 @@ import helpers as H
 import oracle as O
 from qphix_b200 import fields, layout, ops
 from qphix_b200.halo import GPUKernels, face_kind, local_geometry
-from qphix_b200.lattice import BF16, F16, F16N, F32, F64, Geometry
+from qphix_b200.lattice import BF16, F16, F16N, F32, F64, FTYPE_NAMES, Geometry
 
 pytestmark = pytest.mark.gpu
-TOL = {F32: 2e-6, F64: 1e-13, F16: 1e-3, F16N: 2e-3, BF16: 1e-2}
+TOL = H.TOL
 LAYOUTS = [(1, 1, F32), (4, 16, F32), (16, 16, F32), (2, 4, F64), (8, 8, F16), (8, 8, F16N), (4, 16, BF16)]
 
 
@@ -34,9 +35,10 @@ def test_face_pack(cuda, soa, vec, ft):
         for isign in (1, -1):
             buf = torch.zeros(g.face_elems * g.face_sites(d), dtype=g.dtype, device=cuda)
             ops.face_pack(g, isign, 1, psi, buf, d)
-            ref = O.face_pack(g, isign, 1, f["psi"], d)
-            a, r = _face_values(g, buf), _face_values(g, H.to_torch(ref))
-            assert np.abs(a - r).max() <= TOL[ft] * np.abs(r).max() * 4, (d, isign)
+            ref = O.face_pack(g, isign, 1, f["psi"], d, fp64_out=True)
+            e = H.record("face pack %s soa%d" % (FTYPE_NAMES[ft], soa), H.face_rel_err(_face_values(g, buf), ref),
+                         TOL[ft])
+            assert e < TOL[ft], (d, isign, e)
 
 
 @pytest.mark.parametrize("soa,vec,ft", LAYOUTS)
@@ -59,11 +61,12 @@ def test_face_unpack(cuda, soa, vec, ft):
                 out = H.to_torch(f["chi"], cuda)
                 ops.face_unpack(g, fam, isign, 0, H.to_torch(inbuf_np, cuda), gauge, out, d, beta=0.41,
                                 clover=cl, mu=pp["mu"], muinv=pp["muinv"], tbc=tbc, tbc_phases=pp["tbc_phases"])
-                ref = O.face_unpack(g, fam, isign, 0, inbuf_np, f["gauge"], f["chi"].copy(), d, beta=0.41,
+                ref = O.face_unpack(g, fam, isign, 0, inbuf_np, f["gauge"], H.as_f64(g, f["chi"]), d, beta=0.41,
                                     clover=cl_np, mu=pp["mu"], muinv=pp["muinv"], tbc=tbc,
-                                    tbc_phases=pp["tbc_phases"])
+                                    tbc_phases=pp["tbc_phases"], fp64_out=True)
                 assert n * g.face_elems == inbuf_np.size
-                e = H.site_rel_err(g, H.to_np(out), ref)
+                e = H.site_rel_err(g, H.to_np(out), ref, g.with_(ftype=F64))
+                H.record("face unpack %s soa%d" % (FTYPE_NAMES[ft], soa), e, TOL[ft])
                 assert e < TOL[ft], (fam, d, isign, e)
 
 
@@ -123,4 +126,5 @@ def test_two_slab_decomposition_on_one_gpu(cuda, ft):
                     got = layout.unpack_spinor(g, out.cpu())
                     exp = ref_c[r * g.nt:(r + 1) * g.nt]
                     err = float((got - exp).abs().max() / exp.abs().max())
-                    assert err < (2e-6 if ft == F32 else 1e-13), (fam, kernel, isign, r, err)
+                    H.record("two t slabs vs whole lattice %s" % FTYPE_NAMES[ft], err, TOL[ft])
+                    assert err < TOL[ft], (fam, kernel, isign, r, err)

@@ -98,3 +98,29 @@ def test_mrhs_reliable_updates(cuda, lo, nrhs, family):
         assert np.linalg.norm(ff["b"] - mx) / np.linalg.norm(ff["b"]) < 2e-10
     _, dc = mrhs.mixed_solve(op64, oplo, bs, tol=1e-10, inner_tol=1e-2)
     assert info["inner_iters"] <= dc["inner_iters"] + 5, (info, dc)
+
+
+@pytest.mark.parametrize("solver", ["cg_reliable", "cg"])
+def test_mrhs_zero_source(cuda, solver):
+    """One zero source among eight: its solution stays exactly zero and the
+    other seven still reach 1e-10 (a zero residual must not turn the
+    recurrence coefficients into 0/0)."""
+    family, nrhs = "clover", 8
+    g = Geometry(8, 8, 8, 8, soalen=4, veclen=8, ftype=F64, compress12=True, t_boundary=-1.0)
+    f, p = H.eo_setup(g, family)
+    op64 = _ops(g, family, f, p, cuda)
+    g16 = g.with_(ftype=F16)
+    op16 = _ops(g16, family, f, p, cuda, dtype=torch.float16)
+    rng = np.random.default_rng(31)
+    bs = [torch.from_numpy(rng.normal(size=g.spinor_elems)).to(cuda) for _ in range(nrhs)]
+    bs[3] = torch.zeros_like(bs[3])
+    xs, info = mrhs.mixed_solve(op64, op16, bs, tol=1e-10, inner_tol=1e-2, solver=solver)
+    assert all(np.isfinite(info["rel_res"])), info
+    assert max(info["rel_res"]) <= 1e-10, info
+    assert torch.count_nonzero(xs[3]) == 0
+    for i, (b, x) in enumerate(zip(bs, xs)):
+        if i == 3:
+            continue
+        ff = dict(f, b=b.cpu().numpy())
+        mx = H.oracle_schur(g, family, ff, p, x.cpu().numpy())
+        assert np.linalg.norm(ff["b"] - mx) / np.linalg.norm(ff["b"]) < 2e-10

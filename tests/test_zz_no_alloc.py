@@ -13,11 +13,11 @@ import pytest
 import torch
 
 import helpers as H
-from qphix_b200 import _lib
-from qphix_b200.lattice import F32, F64, Geometry
+from qphix_b200 import _lib, fields, layout
+from qphix_b200.lattice import F16N, F32, F64, Geometry
 from qphix_b200.solver import EvenOddOperator
 
-TOL = {F32: 2e-6, F64: 1e-13}
+TOL = H.TOL
 
 
 def _operator(g, family, dev, seed):
@@ -29,15 +29,16 @@ def _operator(g, family, dev, seed):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("ft,family", [(F32, "clover"), (F64, "tm_clover")])
+# FP16 + per-site norm has 26 stored halves per site (the norm included), not
+# the 24 elements of the other types: the scratch-size check must count them
+@pytest.mark.parametrize("ft,family", [(F32, "clover"), (F64, "tm_clover"), (F16N, "tm")])
 def test_noalloc_matches_caller_scratch_twice(cuda, ft, family):
     L = _lib.lib()
     g = Geometry(16, 16, 8, 8, soalen=8, veclen=8, ftype=ft, compress12=True, t_boundary=-1.0)
     op, f = _operator(g, family, cuda, seed=700)
-    rng = np.random.default_rng(11)
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     for call, isign in enumerate((1, -1)):
-        src = torch.from_numpy(rng.normal(size=g.spinor_elems).astype(f["b"].dtype)).to(cuda)
+        src = H.to_torch(layout.pack_spinor(g, fields.random_spinor(g, seed=710 + call)), cuda)
         out_na = torch.full_like(src, float("nan"))
         rc = L.qb200_schur_apply_noalloc(ctypes.byref(op.lat), ctypes.byref(op.op), isign,
                                          ctypes.c_void_p(src.data_ptr()), ctypes.c_void_p(out_na.data_ptr()),
@@ -49,7 +50,7 @@ def test_noalloc_matches_caller_scratch_twice(cuda, ft, family):
                                  ctypes.c_void_p(out_ref.data_ptr()), ctypes.c_void_p(tmp.data_ptr()), stream)
         _lib.check(rc)
         torch.cuda.synchronize()
-        e = H.site_rel_err(g, out_na.cpu().numpy(), out_ref.cpu().numpy())
+        e = H.site_rel_err(g, H.to_np(out_na), H.to_np(out_ref))
         assert e < TOL[ft], (call, e)
 
 
