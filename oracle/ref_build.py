@@ -263,6 +263,25 @@ def build(name, jobs=8, opt="-O2"):
     return so
 
 
+def render_decls():
+    """Render the reference's kernel declaration templates
+    (codegen/jinja/{dslash,clov_dslash,tm_dslash,tm_clov_dslash}_decl.h.j2,
+    unchanged, with jinja2 as codegen/jinja/generate_files.py does) and copy
+    its Types<> header (codegen/include/decl_common.h) into
+    oracle/_ref/include/, for the tests that compile a QPhiX-style caller
+    against them and link the B200 library's per-tile kernels."""
+    import jinja2
+    inc = os.path.join(OUT, "include")
+    os.makedirs(inc, exist_ok=True)
+    env = jinja2.Environment(loader=jinja2.FileSystemLoader(REF))
+    for k in ("dslash", "clov_dslash", "tm_dslash", "tm_clov_dslash"):
+        text = env.get_template("jinja/%s_decl.h.j2" % k).render()
+        with open(os.path.join(inc, "%s_decl.h" % k), "w") as f:
+            f.write("#pragma once\n" + text)
+    shutil.copy(os.path.join(REF, "include", "decl_common.h"), os.path.join(inc, "decl_common.h"))
+    return inc
+
+
 def main(argv):
     argv = list(argv)
     explicit = None
@@ -275,6 +294,7 @@ def main(argv):
         print("reference sources not present; using prebuilt oracle/_ref if any")
         return 0
     set_reference(root)
+    print("rendered the reference's kernel declarations into", render_decls(), flush=True)
     names = argv or DEFAULT
     for n in names:
         print("building", n, "->", build(n), flush=True)

@@ -43,7 +43,8 @@ def units():
            (os.path.join(BUILD, "qb200_mrhs.o"), [], os.path.join(CSRC, "qb200_mrhs.cu")),
            (os.path.join(BUILD, "qb200_force.o"), [], os.path.join(CSRC, "qb200_force.cu")),
            (os.path.join(BUILD, "qb200_batch.o"), [], os.path.join(CSRC, "qb200_batch.cu")),
-           (os.path.join(BUILD, "qb200_convert.o"), [], os.path.join(CSRC, "qb200_convert.cu"))]
+           (os.path.join(BUILD, "qb200_convert.o"), [], os.path.join(CSRC, "qb200_convert.cu")),
+           (os.path.join(BUILD, "qb200_qphix_tiles.o"), [], os.path.join(CSRC, "qb200_qphix_tiles.cu"))]
     for tag, ft in FTYPES.items():
         for s in SOALENS:
             if tag in WIDE_ONLY and s < 4:

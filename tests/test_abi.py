@@ -10,13 +10,18 @@ import pytest
 from qphix_b200 import _lib
 from qphix_b200.lattice import BF16, F16N, F32, Geometry
 
-HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "qphix_b200.h")
+INCLUDE = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+HEADERS = [os.path.join(INCLUDE, f) for f in sorted(os.listdir(INCLUDE)) if f.endswith(".h")]
 
 
 def declared_symbols():
-    src = open(HEADER).read()
-    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(qb200_[a-z0-9_]+)\s*\(", src)))
+    """every extern "C" entry point of include/*.h (the QPhiX template
+    specialisations of qphix_b200_qphix.h are checked by test_qphix_tiles)"""
+    syms = set()
+    for h in HEADERS:
+        src = re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
+        syms.update(re.findall(r"\b(qb200_[a-z0-9_]+)\s*\(", src))
+    return sorted(syms)
 
 
 def test_header_declares_the_reference_kernel_set():
