@@ -48,10 +48,12 @@ def parse():
     ap.add_argument("--veclen", type=int, default=0)
     ap.add_argument("--dims", default="32,32,32,64")
     ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--nrhs", type=int, default=8, help="right-hand sides of --only solve_tm_mrhs")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bound of the CPU baseline sample")
     ap.add_argument("--no-extras", action="store_true", help="skip the multi-RHS and solver measurements")
-    ap.add_argument("--only", choices=["mrhs", "force", "batch", "solve", "tm", "solve_tm", "solve_tm_clover"],
+    ap.add_argument("--only", choices=["mrhs", "force", "batch", "solve", "tm", "solve_tm", "solve_tm_clover",
+                                       "solve_tm_mrhs"],
                     help="run one secondary measurement alone (on --dims) and print its JSON line")
     return ap.parse_args()
 
@@ -427,6 +429,62 @@ def bench_solve_tm(dev, dims=(48, 48, 48, 96), kappa=0.16, mu=0.01, family="tm")
                                   "updates": rr_[1]["outer_iters"], "rel_res": true_res(rr_[0])}
     out["speedup_vs_fp64_cg"] = t64 / tr
     out["speedup_vs_fp32_fp64_mixed"] = t32 / tr
+    return out
+
+
+def bench_solve_tm_mrhs(dev, dims=(48, 48, 48, 96), kappa=0.16, mu=0.01, nrhs=8):
+    """The even-odd twisted-mass system of bench_solve_tm (48^3x96, kappa =
+    0.16, mu = 0.01, 12-real links, SOALEN 8) for nrhs Gaussian sources to
+    |b - Mhat x|/|b| <= 1e-10: (a) the single-RHS FP32 CG corrected in FP64,
+    source by source, against (b) all sources in one FP16-storage multi-RHS
+    CG with FP64 reliable updates (links FP16, each right-hand side scaled
+    to unit norm in its FP16 slot).  Every solution's residual is recomputed
+    with the FP64 operator.  One untimed run of each path on a loose
+    tolerance, then three timed runs; the median is reported."""
+    from qphix_b200 import fields, layout, mrhs
+    from qphix_b200.lattice import F16, F32, F64, Geometry
+    from qphix_b200.solver import EvenOddOperator, mixed_solve
+    G = Geometry(*dims, soalen=8, veclen=8, compress12=True, t_boundary=-1.0, ftype=F64)
+    U = fields.random_gauge(G, seed=177, device=dev)
+    gauge = [layout.pack_gauge(G, U, cb, torch.float64) for cb in (0, 1)]
+    del U
+    alpha = 1.0 / (2 * kappa)
+    p = dict(coeff_s=0.5, coeff_t_f=0.5, coeff_t_b=0.5, alpha=alpha, mu=mu / alpha,
+             muinv=alpha / (alpha ** 2 + mu ** 2))
+    ops_ = {}
+    for ft, dt in ((F64, torch.float64), (F32, torch.float32), (F16, torch.float16)):
+        ops_[ft] = EvenOddOperator(G.with_(ftype=ft), "tm", gauge=[x.to(dt) for x in gauge], target_cb=1, **p)
+    del gauge
+    bs = [layout.pack_spinor(G, fields.random_spinor(G, seed=281 + i, device=dev), torch.float64)
+          for i in range(nrhs)]
+    out = {"lattice": list(dims), "family": "tm", "kappa": kappa, "mu": mu, "tol": 1e-10, "nrhs": nrhs,
+           "soalen": 8, "inner_storage": "fp16 multi-RHS (links fp16, 12-real)"}
+    mixed_solve(ops_[F64], ops_[F32], bs[0], tol=1e-4, inner_tol=1e-2)
+    mrhs.mixed_solve(ops_[F64], ops_[F16], bs, tol=1e-3, inner_tol=1e-2, solver="cg_reliable")
+
+    def timed(fn, reps=3):
+        ts = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return statistics.median(ts), r, ts
+
+    def true_res(b, x):
+        return float((b - ops_[F64].apply(x)).norm() / b.norm())
+
+    t32, r32, a32 = timed(lambda: [mixed_solve(ops_[F64], ops_[F32], b, tol=1e-10, inner_tol=1e-5) for b in bs])
+    out["fp32_fp64_single_rhs"] = {"seconds": t32, "runs": a32, "inner_iters": [r[1]["inner_iters"] for r in r32],
+                                   "max_rel_res": max(true_res(b, r[0]) for b, r in zip(bs, r32))}
+    del r32
+    tr, rr_, ar = timed(lambda: mrhs.mixed_solve(ops_[F64], ops_[F16], bs, tol=1e-10, inner_tol=1e-2,
+                                                 solver="cg_reliable"))
+    out["fp16_multi_rhs_reliable"] = {"seconds": tr, "runs": ar, "iters": rr_[1]["inner_iters"],
+                                      "updates": rr_[1]["outer_iters"],
+                                      "max_rel_res": max(true_res(b, x) for b, x in zip(bs, rr_[0]))}
+    out["speedup_vs_fp32_fp64_single_rhs"] = t32 / tr
     return out
 
 
@@ -830,6 +888,7 @@ def b200_arm(args, world, rank, local):
         extras["tm_fp16n"] = bench_tm(dev)
         extras["solve_tm"] = bench_solve_tm(dev)
         extras["solve_tm_clover"] = bench_solve_tm(dev, family="tm_clover")
+        extras["solve_tm_mrhs"] = bench_solve_tm_mrhs(dev)
 
     if rank == 0:
         line = {
@@ -876,6 +935,8 @@ def run_only(args):
         r = bench_solve_tm(dev, dims)
     elif args.only == "solve_tm_clover":
         r = bench_solve_tm(dev, dims, family="tm_clover")
+    elif args.only == "solve_tm_mrhs":
+        r = bench_solve_tm_mrhs(dev, dims, nrhs=args.nrhs)
     else:
         r = bench_solve(dims, dev)
     print(json.dumps({"only": args.only, "dims": list(dims), "result": r}))

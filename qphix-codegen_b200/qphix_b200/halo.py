@@ -1,29 +1,39 @@
-"""T-slab domain decomposition of the dslash over ranks (one GPU per rank).
+"""Domain decomposition of the dslash over a z x t grid of ranks (one GPU
+per rank): t slabs first, then z (pz x pt ranks; pz = 1 gives plain t
+slabs).
 
-Each rank holds a local lattice of nt time slices; rank r owns global slices
-[r*nt, (r+1)*nt).  One application of an operator on checkerboard cb is
+Rank r sits at grid coordinates (rz, rt) = (r % pz, r // pz) and holds the
+local lattice of nz = NZ/pz slices in z and nt = NT/pt slices in t starting
+at z0 = rz*nz, t0 = rt*nt (both even, so local and global checkerboards
+agree).  One application of an operator on checkerboard cb is, for every
+split dimension mu (z: dirs 4, 5; t: dirs 6, 7):
 
-  1. face_proj_dir (dir 7 and 6): project the t = nt-1 and t = 0 sites of psi
-     for the forward / backward neighbour (codegen/dslash.cc:433-458);
-  2. exchange the two face buffers with ranks r+1 and r-1;
-  3. body kernel with accumulate[6] = accumulate[7] = 0: every hop except
-     the ones that leave the slab (this overlaps step 2);
-  4. face_*finish_dir (dir 6 and 7): add the received faces
+  1. face_proj_dir (dirs 2mu+1 and 2mu): project the sites of psi on the
+     forward / backward face for the neighbour beyond it
+     (codegen/dslash.cc:433-458);
+  2. exchange the face buffers with the two neighbours along mu;
+  3. body kernel with accumulate[2mu] = accumulate[2mu+1] = 0 for every split
+     mu: every hop except the ones that leave the local block (this overlaps
+     step 2);
+  4. face_*finish_dir (dirs 2mu and 2mu+1): add the received faces
      (codegen/dslash.cc:463-553).
 
-The face kernels of the reference subtract beta*hop for Wilson and twisted
-mass and add beta*A*hop for clover / TM clover (dslash_common.cc:1975-1981),
-so each (family, kernel) pair maps to one face kind and a sign of beta (see
-`face_kind`).  The time-boundary factor multiplies the beta of the faces that
-cross the global t edge (rank 0 backward, last rank forward).
+The dslash couples nearest neighbours only, so no edge or corner exchange is
+needed.  The face kernels of the reference subtract beta*hop for Wilson and
+twisted mass and add beta*A*hop for clover / TM clover
+(dslash_common.cc:1975-1981), so each (family, kernel) pair maps to one face
+kind and a sign of beta (see `face_kind`).  The beta of a z face is coeff_s;
+a t face gets coeff_t_b / coeff_t_f, times the time-boundary factor on the
+faces that cross the global t edge (grid row rt = 0 backward, rt = pt-1
+forward).
 
 The compute steps are delegated to a `kernels` object (GPU kernels through
-the C-ABI, or the CPU oracle in the tests) and the exchange to `TComm`, so the
-same orchestration runs over NCCL on GPUs and over gloo on CPU.
+the C-ABI, or the CPU oracle in the tests) and the exchange to `GridComm`, so
+the same orchestration runs over NCCL on GPUs and over gloo on CPU.
 
 `TSlabEvenOdd` composes two such applications into the even-odd operator
 Mhat (the composition of qb200_schur_apply), and `cg` solves Mhat^dag Mhat
-x = Mhat^dag b over the slabs: vectors stay local, each inner product is a
+x = Mhat^dag b over the blocks: vectors stay local, each inner product is a
 local FP64 sum followed by an all-reduce of the FP64 scalar.
 """
 import math
@@ -42,31 +52,43 @@ def face_kind(family, kernel):
             "tm": ("tm", -1.0), "tm_clover": ("tm_clover", 1.0)}[family]
 
 
-class TComm:
-    """Nearest-neighbour exchange along t over torch.distributed."""
+class GridComm:
+    """Nearest-neighbour exchange on a pz x pt grid of ranks over
+    torch.distributed (rank = rt * pz + rz).  pz = None: every rank in t."""
 
-    def __init__(self, group=None):
+    def __init__(self, pz=None, group=None):
         self.group = group
         self.rank = dist.get_rank(group) if dist.is_initialized() else 0
         self.world = dist.get_world_size(group) if dist.is_initialized() else 1
+        self.pz = 1 if pz is None else int(pz)
+        if self.pz < 1 or self.world % self.pz:
+            raise ValueError("pz = %d does not divide the %d ranks" % (self.pz, self.world))
+        self.pt = self.world // self.pz
+        self.rz, self.rt = self.rank % self.pz, self.rank // self.pz
         nccl = dist.is_initialized() and dist.get_backend(group) == "nccl"
         self.device = torch.device("cuda", torch.cuda.current_device()) if nccl else torch.device("cpu")
 
-    @property
-    def fwd(self):
-        return (self.rank + 1) % self.world
+    def parts(self, mu):
+        """ranks along dimension mu (2 = z, 3 = t; x and y are never split)"""
+        return {2: self.pz, 3: self.pt}.get(mu, 1)
 
-    @property
-    def back(self):
-        return (self.rank - 1) % self.world
+    def neighbour(self, mu, step):
+        rz, rt = self.rz, self.rt
+        if mu == 2:
+            rz = (rz + step) % self.pz
+        else:
+            rt = (rt + step) % self.pt
+        return rt * self.pz + rz
 
-    def start(self, send_fwd, send_back, recv_from_back, recv_from_fwd):
-        """Post the four transfers; returns the request handles."""
-        g = self.group
-        ops = [dist.P2POp(dist.isend, send_fwd, self._peer(self.fwd), g, tag=0),
-               dist.P2POp(dist.irecv, recv_from_back, self._peer(self.back), g, tag=0),
-               dist.P2POp(dist.isend, send_back, self._peer(self.back), g, tag=1),
-               dist.P2POp(dist.irecv, recv_from_fwd, self._peer(self.fwd), g, tag=1)]
+    def start(self, mu, send_fwd, send_back, recv_from_back, recv_from_fwd):
+        """Post the four transfers along mu; returns the request handles.
+        With two ranks along mu both neighbours are the same rank: the two
+        messages each way are told apart by tag (gloo) and by order (NCCL)."""
+        g, fwd, back = self.group, self.neighbour(mu, 1), self.neighbour(mu, -1)
+        ops = [dist.P2POp(dist.isend, send_fwd, self._peer(fwd), g, tag=2 * mu),
+               dist.P2POp(dist.irecv, recv_from_back, self._peer(back), g, tag=2 * mu),
+               dist.P2POp(dist.isend, send_back, self._peer(back), g, tag=2 * mu + 1),
+               dist.P2POp(dist.irecv, recv_from_fwd, self._peer(fwd), g, tag=2 * mu + 1)]
         return dist.batch_isend_irecv(ops)
 
     def _peer(self, r):
@@ -86,22 +108,49 @@ class TComm:
             r.wait()
 
 
+class TComm(GridComm):
+    """Every rank along t (pz = 1): the t-slab decomposition."""
+
+    def __init__(self, group=None):
+        super().__init__(1, group)
+
+    @property
+    def fwd(self):
+        return self.neighbour(3, 1)
+
+    @property
+    def back(self):
+        return self.neighbour(3, -1)
+
+
+def grid_geometry(g_global: Geometry, rank, pz, pt) -> Geometry:
+    """The block of `rank` (rz = rank % pz, rt = rank // pz) of a lattice
+    split into pz x pt equal blocks in z and t."""
+    if g_global.nz % pz or (g_global.nz // pz) % 2:
+        raise ValueError("nz = %d must split into even blocks over %d ranks" % (g_global.nz, pz))
+    if g_global.nt % pt or (g_global.nt // pt) % 2:
+        raise ValueError("nt = %d must split into even slabs over %d ranks" % (g_global.nt, pt))
+    rt = rank // pz
+    return g_global.with_(nz=g_global.nz // pz, nt=g_global.nt // pt, t_edge_lo=(rt == 0),
+                          t_edge_hi=(rt == pt - 1))
+
+
 def local_geometry(g_global: Geometry, rank, world) -> Geometry:
     """The slab of `rank` of a lattice split into `world` equal t slabs."""
-    if g_global.nt % world or (g_global.nt // world) % 2:
-        raise ValueError("nt = %d must split into even slabs over %d ranks" % (g_global.nt, world))
-    return g_global.with_(nt=g_global.nt // world, t_edge_lo=(rank == 0), t_edge_hi=(rank == world - 1))
+    return grid_geometry(g_global, rank, 1, world)
 
 
-class TSlabDslash:
-    """Operator application on a t slab with halo exchange."""
+class HaloDslash:
+    """Operator application on a z x t block with halo exchange."""
 
-    def __init__(self, g: Geometry, comm: TComm, kernels):
+    def __init__(self, g: Geometry, comm: GridComm, kernels):
         self.g = g
         self.comm = comm
         self.k = kernels
-        nface = g.face_sites(6)
-        self.bufs = [kernels.alloc(g.face_elems * nface) for _ in range(4)]  # send fwd, send back, recv back, recv fwd
+        self.split = [mu for mu in (2, 3) if comm.parts(mu) > 1]
+        # per split mu: send fwd, send back, recv from back, recv from fwd
+        self.bufs = {mu: [kernels.alloc(g.face_elems * g.face_sites(2 * mu)) for _ in range(4)]
+                     for mu in self.split}
 
     def apply(self, family, kernel, isign, cb, psi, out, gauge, chi=None, clover=None, coeff_s=1.0,
               coeff_t_f=1.0, coeff_t_b=1.0, alpha=1.0, mu=0.0, muinv=1.0, rho=0.0, tbc_mask=0,
@@ -109,26 +158,39 @@ class TSlabDslash:
         g = self.g
         kw = dict(chi=chi, clover=clover, coeff_s=coeff_s, coeff_t_f=coeff_t_f, coeff_t_b=coeff_t_b,
                   alpha=alpha, mu=mu, muinv=muinv, rho=rho, tbc_mask=tbc_mask, tbc_phases=tbc_phases)
-        if self.comm.world == 1:
+        if not self.split:
             self.k.body(g, family, kernel, isign, cb, psi, out, gauge, accumulate=None, **kw)
             return out
-        send_fwd, send_back, recv_back, recv_fwd = self.bufs
-        self.k.pack(g, isign, 1 - cb, psi, send_fwd, 7)
-        self.k.pack(g, isign, 1 - cb, psi, send_back, 6)
-        reqs = self.comm.start(send_fwd, send_back, recv_back, recv_fwd)
-        self.k.body(g, family, kernel, isign, cb, psi, out, gauge, accumulate=[1, 1, 1, 1, 1, 1, 0, 0], **kw)
+        reqs = []
+        acc = [1] * 8
+        for d in self.split:
+            send_fwd, send_back, recv_back, recv_fwd = self.bufs[d]
+            self.k.pack(g, isign, 1 - cb, psi, send_fwd, 2 * d + 1)
+            self.k.pack(g, isign, 1 - cb, psi, send_back, 2 * d)
+            reqs += self.comm.start(d, send_fwd, send_back, recv_back, recv_fwd)
+            acc[2 * d] = acc[2 * d + 1] = 0
+        self.k.body(g, family, kernel, isign, cb, psi, out, gauge, accumulate=acc, **kw)
         self.comm.wait(reqs)
         fam, sg = face_kind(family, kernel)
         tb = g.t_boundary
-        beta_b = sg * coeff_t_b * (tb if g.t_edge_lo else 1.0)
-        beta_f = sg * coeff_t_f * (tb if g.t_edge_hi else 1.0)
-        tbc = bool(tbc_mask & 8)
         cl = clover if fam in ("clover", "tm_clover") else None
-        self.k.unpack(g, fam, isign, cb, recv_back, gauge, out, 6, beta=beta_b, clover=cl, mu=mu, muinv=muinv,
-                      tbc=tbc, tbc_phases=tbc_phases)
-        self.k.unpack(g, fam, isign, cb, recv_fwd, gauge, out, 7, beta=beta_f, clover=cl, mu=mu, muinv=muinv,
-                      tbc=tbc, tbc_phases=tbc_phases)
+        for d in self.split:
+            _, _, recv_back, recv_fwd = self.bufs[d]
+            if d == 3:
+                beta_b = sg * coeff_t_b * (tb if g.t_edge_lo else 1.0)
+                beta_f = sg * coeff_t_f * (tb if g.t_edge_hi else 1.0)
+            else:
+                beta_b = beta_f = sg * coeff_s
+            tbc = bool(tbc_mask & (1 << d))
+            self.k.unpack(g, fam, isign, cb, recv_back, gauge, out, 2 * d, beta=beta_b, clover=cl, mu=mu,
+                          muinv=muinv, tbc=tbc, tbc_phases=tbc_phases)
+            self.k.unpack(g, fam, isign, cb, recv_fwd, gauge, out, 2 * d + 1, beta=beta_f, clover=cl, mu=mu,
+                          muinv=muinv, tbc=tbc, tbc_phases=tbc_phases)
         return out
+
+
+# the t-slab form (a GridComm with pz = 1 splits t only)
+TSlabDslash = HaloDslash
 
 
 class TSlabEvenOdd:

@@ -92,14 +92,16 @@ def unpack_spinor(g: Geometry, flat: torch.Tensor) -> torch.Tensor:
     return torch.view_as_complex(b)
 
 
-def site_links(g: Geometry, U: torch.Tensor, cb: int, t0: int = 0) -> torch.Tensor:
+def site_links(g: Geometry, U: torch.Tensor, cb: int, t0: int = 0, z0: int = 0) -> torch.Tensor:
     """The eight links each site of cb uses, as U (not transposed):
-    (nt, nz, ny, nxh, 8, 3, 3).  U may cover a longer time extent than g
-    (a global lattice of which g is the slab starting at time slice t0)."""
+    (nt, nz, ny, nxh, 8, 3, 3).  U may cover longer z and t extents than g
+    (a global lattice of which g is the block starting at slices z0, t0;
+    both even, so that local and global checkerboards agree)."""
     x, y, z, t = cb_coords(g, cb, U.device)
-    NT = U.shape[1]
+    NZ, NT = U.shape[2], U.shape[1]
     t = (t + t0) % NT
-    L = [g.nx, g.ny, g.nz, NT]
+    z = (z + z0) % NZ
+    L = [g.nx, g.ny, NZ, NT]
     links = []
     for mu in range(4):
         c = [x, y, z, t]
@@ -125,11 +127,11 @@ def _from_tiles(g: Geometry, flat: torch.Tensor, K: int) -> torch.Tensor:
     return v.reshape(g.nt, g.nz, g.ny, g.nxh, K)
 
 
-def pack_gauge(g: Geometry, U: torch.Tensor, cb: int, dtype=None, t0: int = 0) -> torch.Tensor:
+def pack_gauge(g: Geometry, U: torch.Tensor, cb: int, dtype=None, t0: int = 0, z0: int = 0) -> torch.Tensor:
     """Full-lattice links -> SU3MatrixBlock array of checkerboard cb (of the
-    slab of g that starts at global time slice t0)."""
+    block of g that starts at global slices z0 and t0)."""
     dtype = dtype or g.dtype
-    G = site_links(g, U.to(torch.complex128), cb, t0).transpose(-1, -2)   # G = U^T
+    G = site_links(g, U.to(torch.complex128), cb, t0, z0).transpose(-1, -2)   # G = U^T
     G = G[..., : g.rows, :]
     r = torch.view_as_real(G.resolve_conj()).reshape(g.nt, g.nz, g.ny, g.nxh, 8 * g.rows * 6)
     return _to_tiles(g, r).to(dtype).contiguous()
