@@ -96,29 +96,41 @@ def test_wilson_hop_fp32_forward_fp64_check(cuda):
         assert float((a - b).abs().max()) <= 2e-5 * float(b.abs().max())
 
 
-@pytest.mark.parametrize("family", ["clover", "wilson", "tm"])
+def _pseudofermion_fd(cuda, g, family, seed, tol=1e-14):
+    """dS/dU of S = phi^dag (Mhat^dag Mhat)^-1 phi along NDIR random su(3)
+    directions against central differences (FP64, CG to tol); returns the
+    worst |analytic - fd| / max(1, |fd|)."""
+    f, p = H.eo_setup(g, family, seed=seed, kappa=0.11)
+    U = fields.random_gauge(g, seed=seed, device=cuda).requires_grad_(True)
+    phi = H.to_torch(f["b"], cuda)
+    T = lambda cs: tuple(H.to_torch(c, cuda) if c is not None else None for c in cs)
+    clov, clov_dag = T(f["clov"]), T(f["clov_dag"])
+    kw = dict(p, target_cb=1)
+    S = AG.PseudofermionAction.apply(U, phi, g, family, kw, clov, clov_dag, tol)
+    S.backward()
+    Ud = U.detach()
+    worst = 0.0
+    with torch.no_grad():
+        for k in range(NDIR):
+            X = H.random_algebra(Ud.shape[:-2], seed=720 + k)
+            sp = float(AG.PseudofermionAction.apply(H.moved_links(Ud, X, EPS), phi, g, family, kw, clov, clov_dag,
+                                                    tol))
+            sm = float(AG.PseudofermionAction.apply(H.moved_links(Ud, X, -EPS), phi, g, family, kw, clov, clov_dag,
+                                                    tol))
+            fd = (sp - sm) / (2 * EPS)
+            an = H.directional(U.grad, X, Ud)
+            worst = max(worst, abs(an - fd) / max(1.0, abs(fd)))
+    return worst
+
+
+@pytest.mark.parametrize("family", ["clover", "wilson", "tm", "tm_clover"])
 def test_pseudofermion_action_fd(cuda, family):
     """S = phi^dag (Mhat^dag Mhat)^-1 phi: dS/dU along 8 random su(3)
     directions against central differences (FP64, CG to 1e-14)."""
     g = Geometry(8, 4, 4, 4, soalen=4, ftype=F64, t_boundary=-1.0)
-    f, p = H.eo_setup(g, family, seed=640, kappa=0.11)
-    U = fields.random_gauge(g, seed=640).to(cuda).requires_grad_(True)
-    phi = H.to_torch(f["b"], cuda)
-    clov = tuple(H.to_torch(c, cuda) if c is not None else None for c in f["clov"])
-    kw = dict(p, target_cb=1)
-    S = AG.PseudofermionAction.apply(U, phi, g, family, kw, clov, (None, None), 1e-14)
-    S.backward()
-    Ud = U.detach()
-    with torch.no_grad():
-        for k in range(NDIR):
-            X = H.random_algebra(Ud.shape[:-2], seed=720 + k)
-            sp = float(AG.PseudofermionAction.apply(H.moved_links(Ud, X, EPS), phi, g, family, kw, clov,
-                                                    (None, None), 1e-14))
-            sm = float(AG.PseudofermionAction.apply(H.moved_links(Ud, X, -EPS), phi, g, family, kw, clov,
-                                                    (None, None), 1e-14))
-            fd = (sp - sm) / (2 * EPS)
-            an = H.directional(U.grad, X, Ud)
-            assert abs(an - fd) <= FD_TOL * max(1.0, abs(fd)), (k, an, fd)
+    e = H.record("pseudofermion dS/dU vs central differences (8^3x4 family mix)",
+                 _pseudofermion_fd(cuda, g, family, 640), FD_TOL)
+    assert e <= FD_TOL, (family, e)
 
 
 def test_pseudofermion_phi_grad(cuda):
