@@ -276,17 +276,31 @@ __device__ __forceinline__ void async_body(const KArgs<FT> &a, const GeoDev &g, 
   __syncwarp();
 }
 
-// Grid as site_dslash_kernel (blockIdx.y = the (z, t) plane), blocks of 128
-// threads.  Threads past the plane's last site take part in the warp's
-// copies (on a clamped site) and store nothing.  Needs 16-byte aligned fields
-// smaller than 32 GiB.
+// Work unit: one warp's 32 sites of one (z, t) plane, numbered over all
+// planes (warp_units_per_plane per plane), so that no warp idles when a
+// plane's sites do not fill whole blocks of 128 threads; one-dimensional grid
+// of warp_blocks(g) blocks of 128 threads.  Threads past the plane's last
+// site take part in the warp's copies (on a clamped site) and store nothing.
+// Needs 16-byte aligned fields smaller than 32 GiB.
+__host__ __device__ __forceinline__ int warp_units_per_plane(const GeoDev &g) { return (g.nxh * g.ny + 31) >> 5; }
+__host__ __device__ __forceinline__ long long warp_units(const GeoDev &g)
+{
+  return (long long)warp_units_per_plane(g) * g.nz * g.nt;
+}
+inline long long warp_blocks(const GeoDev &g) { return (warp_units(g) + 3) / 4; }
+
 template <typename FT, int S, bool COMP12, int FAM, bool ACH>
 __global__ void __launch_bounds__(128, 4)
     async_site_kernel(const KArgs<FT> a, const GeoDev g, const OpDev<comp_t<FT>> p)
 {
   __shared__ __align__(16) unsigned char smem[4][AsyncCfg<FT, S, COMP12>::BUF];
-  async_body<FT, S, COMP12, FAM, ACH>(a, g, p, blockIdx.y % g.nz, blockIdx.y / g.nz,
-                                      blockIdx.x * blockDim.x + threadIdx.x, smem[threadIdx.x >> 5]);
+  const long long u = (long long)blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (u >= warp_units(g)) return; // whole warps
+  const int wpp = warp_units_per_plane(g);
+  const int plane = (int)(u / wpp);
+  const int wi = (int)(u - (long long)plane * wpp);
+  async_body<FT, S, COMP12, FAM, ACH>(a, g, p, plane % g.nz, plane / g.nz, wi * 32 + (threadIdx.x & 31),
+                                      smem[threadIdx.x >> 5]);
 }
 
 // Batched form (see batch_staged_kernel): work unit = one warp's 32 sites of

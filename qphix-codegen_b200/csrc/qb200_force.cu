@@ -17,10 +17,12 @@
 // Re tr(X^dag P).  FP32 or FP64 storage, written in the storage type.
 // The reference has no backward kernels; this is an addition of the B200
 // build.
+#include <cstdint>
 #include <cstring>
 #include <string>
 
 #include "qphix_b200.h"
+#include "qb200_async_kernel.cuh"
 #include "qb200_internal.h"
 
 namespace qb200 {
@@ -61,21 +63,18 @@ __device__ __forceinline__ void recons_adj(const cx<C> (&chi)[4][3], C beta, C t
 // Output layout: component k = ((D*3 + a)*3 + b)*2 + ri of site i (the
 // site-th site of cb in (t, z, y, xcb) order) at out[k * nsites + i], so a
 // warp's stores are contiguous.
-template <typename FT, int S, bool PROJ, bool COMP12, int D>
-__device__ __forceinline__ void force_dir(const elem_t<FT> *__restrict__ psi, const elem_t<FT> *__restrict__ gauge,
-                                          const GeoDev &g, const OpDev<comp_t<FT>> &p, const Site &s, long long gbase,
-                                          const cx<comp_t<FT>> (&chi)[4][3], elem_t<FT> *__restrict__ o, int ns)
+//
+// The force of hop D at one site from its neighbour spinor nb, chi, beta and
+// (PROJ) the stored link G of the hop.
+template <typename FT, bool PROJ, int D>
+__device__ __forceinline__ void force_from(const cx<comp_t<FT>> (&nb)[4][3], const cx<comp_t<FT>> (&chi)[4][3],
+                                           const cx<comp_t<FT>> (&G)[3][3], comp_t<FT> beta,
+                                           const OpDev<comp_t<FT>> &p, elem_t<FT> *__restrict__ o, int ns)
 {
   typedef comp_t<FT> C;
   constexpr int MU = D / 2;
   constexpr bool FWD = (D & 1) != 0;
-  bool cross;
-  const Site n = neighbour<D>(g, s, &cross);
-  C beta = p.beta[D];
-  if (D == 6 && s.t == 0 && p.t_edge_lo) beta *= p.tbound;
-  if (D == 7 && s.t == g.nt - 1 && p.t_edge_hi) beta *= p.tbound;
-  cx<C> nb[4][3], b[2][3], h[2][3];
-  load_spinor<FT, S>(psi, spinor_base<FT, S>(g, n), nb);
+  cx<C> b[2][3], h[2][3];
   project<C, D>(nb, p.isPlus ? (C)1 : (C)-1, b);
   const C tau = ((p.isPlus != 0) != FWD) ? (C)1 : (C)-1;
   recons_adj<C, MU>(chi, beta, tau, h);
@@ -114,8 +113,7 @@ __device__ __forceinline__ void force_dir(const elem_t<FT> *__restrict__ psi, co
     }
   if (PROJ) {
     // P = TA(F U^dag), U^dag[k][bb] = conj(U[bb][k]) = conj(G[k][bb])
-    cx<C> G[3][3], M[3][3];
-    load_link<FT, COMP12, D>(gauge, gbase, g.V, G);
+    cx<C> M[3][3];
 #pragma unroll
     for (int a = 0; a < 3; a++)
 #pragma unroll
@@ -145,6 +143,30 @@ __device__ __forceinline__ void force_dir(const elem_t<FT> *__restrict__ psi, co
       ftraits<FT>::st(o + (long long)(((D * 3 + a) * 3 + bb) * 2 + 0) * ns, F[a][bb].re);
       ftraits<FT>::st(o + (long long)(((D * 3 + a) * 3 + bb) * 2 + 1) * ns, F[a][bb].im);
     }
+}
+
+// the hop coefficient of direction D at site s (time-boundary factor included)
+template <typename C, int D>
+__device__ __forceinline__ C force_beta(const GeoDev &g, const OpDev<C> &p, const Site &s)
+{
+  C beta = p.beta[D];
+  if (D == 6 && s.t == 0 && p.t_edge_lo) beta *= p.tbound;
+  if (D == 7 && s.t == g.nt - 1 && p.t_edge_hi) beta *= p.tbound;
+  return beta;
+}
+
+template <typename FT, int S, bool PROJ, bool COMP12, int D>
+__device__ __forceinline__ void force_dir(const elem_t<FT> *__restrict__ psi, const elem_t<FT> *__restrict__ gauge,
+                                          const GeoDev &g, const OpDev<comp_t<FT>> &p, const Site &s, long long gbase,
+                                          const cx<comp_t<FT>> (&chi)[4][3], elem_t<FT> *__restrict__ o, int ns)
+{
+  typedef comp_t<FT> C;
+  bool cross;
+  const Site n = neighbour<D>(g, s, &cross);
+  cx<C> nb[4][3], G[3][3];
+  load_spinor<FT, S>(psi, spinor_base<FT, S>(g, n), nb);
+  if (PROJ) load_link<FT, COMP12, D>(gauge, gbase, g.V, G);
+  force_from<FT, PROJ, D>(nb, chi, G, force_beta<C, D>(g, p, s), p, o, ns);
 }
 
 template <typename FT, int S, bool PROJ, bool COMP12>
@@ -177,6 +199,159 @@ __global__ void __launch_bounds__(128)
   force_dir<FT, S, PROJ, COMP12, 7>(psi, gauge, g, p, s, gbase, ch, o, ns);
 }
 
+// ---- staged form: FP32, VECLEN == SOALEN in {4, 8, 16} -------------------
+//
+// With narrow blocks (SOALEN 4: one spinor component of a block is a
+// 16-byte piece) the thread-per-site kernel's neighbour loads touch 32/S
+// pieces per warp and component and wait one load latency per direction.
+// Here, as in async_site_kernel, a warp owns 32 sites of one (z, t) plane and
+// copies with cp.async, in 16-byte vectors, the blocks its sites need for
+// direction D+1 (the neighbour blocks, or its own blocks of psi for the x
+// directions, and with the projection the direction's link slab) into one of
+// two shared-memory buffers while it computes and stores the force of
+// direction D.  The arithmetic is force_from's; the output is written
+// directly (per component, a warp's stores are 32 consecutive sites).
+template <typename FT, int S, bool PROJ, bool COMP12> struct ForceCfg {
+  typedef Stage<FT, S> St;
+  static constexpr int R = COMP12 ? 2 : 3;
+  static constexpr int SPB = St::SPB * S * (int)sizeof(elem_t<FT>); // spinor block bytes
+  static constexpr int LKB = R * 6 * S * (int)sizeof(elem_t<FT>);   // link slab bytes
+  static constexpr int LKS = St::stride(R * 6);
+  static constexpr int HOP = St::G * (St::SP + (PROJ ? LKS : 0));
+  static constexpr int BUF = 2 * HOP;
+};
+
+template <typename FT, int S> constexpr bool force_async_layout()
+{
+  return (S == 4 || S == 8 || S == 16) && sizeof(elem_t<FT>) == 4;
+}
+
+template <typename FT, int S, bool PROJ, bool COMP12, int D>
+__device__ __forceinline__ void force_prefetch(const elem_t<FT> *__restrict__ psi,
+                                               const elem_t<FT> *__restrict__ gauge, const GeoDev &g, const Site &s,
+                                               long long obase, const WarpCtx &w, unsigned char *buf)
+{
+  typedef ForceCfg<FT, S, PROJ, COMP12> A;
+  typedef Stage<FT, S> St;
+  bool cross;
+  const long long nbase = obase + neighbour_offset<S, D>(g, s, (long long)St::SPB * S, 1, &cross);
+  stage_in_async<FT, S, A::SPB, St::SP>(psi, D < 2 ? w.own : nbase - w.lane, buf, w.ln);
+  if (PROJ)
+    stage_in_async<FT, S, A::LKB, A::LKS>(gauge, w.tile * (8LL * A::R * 6 * S) + (long long)D * A::R * 6 * S,
+                                          buf + St::G * St::SP, w.ln);
+}
+
+// one pipeline step: issue direction D+1, wait for D, read D's neighbour
+// (and link) from shared memory, then compute and store D's force
+template <typename FT, int S, bool PROJ, bool COMP12, int D>
+__device__ __forceinline__ void force_step(const elem_t<FT> *__restrict__ psi, const elem_t<FT> *__restrict__ gauge,
+                                           const GeoDev &g, const OpDev<comp_t<FT>> &p, const Site &s,
+                                           long long obase, const WarpCtx &w, const cx<comp_t<FT>> (&chi)[4][3],
+                                           elem_t<FT> *__restrict__ o, int ns, bool active)
+{
+  typedef comp_t<FT> C;
+  typedef ForceCfg<FT, S, PROJ, COMP12> A;
+  typedef Stage<FT, S> St;
+  if (D < 7) {
+    force_prefetch<FT, S, PROJ, COMP12, (D < 7 ? D + 1 : 7)>(psi, gauge, g, s, obase, w,
+                                                             w.buf + ((D + 1) & 1) * A::HOP);
+    cp_async_commit();
+    cp_async_wait<1>();
+  } else {
+    cp_async_wait<0>();
+  }
+  __syncwarp();
+  const unsigned char *buf = w.buf + (D & 1) * A::HOP;
+  cx<C> nb[4][3], G[3][3];
+  if (D < 2) {
+    // the x neighbour: in the warp's own blocks of psi, else (a row end
+    // beyond the warp's blocks) read directly
+    bool cross;
+    const long long nbase = obase + neighbour_offset<S, D>(g, s, (long long)St::SPB * S, 1, &cross);
+    const long long nbk = nbase / (St::SPB * S);
+    const int nl = (int)(nbase - nbk * (St::SPB * S));
+    const long long gi = nbk - w.blk0;
+    if (gi >= 0 && gi < St::G) load_spinor_sm<FT, S>(buf + gi * St::SP, nl, nb);
+    else load_spinor<FT, S>(psi, nbase, nb);
+  } else {
+    load_spinor_sm<FT, S>(buf + (w.ln / S) * St::SP, w.lane, nb);
+  }
+  if (PROJ) load_link_sm<FT, S, COMP12>(buf + St::G * St::SP + (w.ln / S) * A::LKS, w.lane, G);
+  __syncwarp();
+  if (active) force_from<FT, PROJ, D>(nb, chi, G, force_beta<C, D>(g, p, s), p, o, ns);
+}
+
+// Work unit: one warp's 32 sites of one (z, t) plane, numbered over all
+// planes (wpp units per plane), so that no warp idles when a plane's sites
+// do not fill whole blocks; lanes past the plane's last site take part in
+// the copies (on a clamped site) and store nothing.  Fields 16-byte aligned,
+// below 32 GiB.
+template <typename FT, int S, bool PROJ, bool COMP12>
+__global__ void __launch_bounds__(128, 4)
+    async_force_kernel(const elem_t<FT> *__restrict__ chi, const elem_t<FT> *__restrict__ psi,
+                       const elem_t<FT> *__restrict__ gauge, elem_t<FT> *__restrict__ out, const GeoDev g,
+                       const OpDev<comp_t<FT>> p)
+{
+  typedef comp_t<FT> C;
+  typedef Stage<FT, S> St;
+  typedef ForceCfg<FT, S, PROJ, COMP12> A;
+  __shared__ __align__(16) unsigned char smem[4][A::BUF];
+  const int nplane = g.nxh * g.ny;
+  const int wpp = (nplane + 31) >> 5;
+  const long long u = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (u >= (long long)wpp * g.nz * g.nt) return; // whole warps
+  const int plane = (int)(u / wpp);
+  const int q0 = (int)(u - (long long)plane * wpp) * 32 + (threadIdx.x & 31);
+  const bool active = q0 < nplane;
+  const int q = active ? q0 : nplane - 1;
+  Site s;
+  s.z = plane % g.nz;
+  s.t = plane / g.nz;
+  s.y = q / g.nxh;
+  s.xcb = q - s.y * g.nxh;
+  s.par = (s.y + s.z + s.t + p.cb) & 1;
+  WarpCtx w;
+  w.buf = smem[threadIdx.x >> 5];
+  w.ln = threadIdx.x & 31;
+  w.tile = tile_of<S>(g, s, &w.lane);
+  const long long obase = spinor_base<FT, S>(g, s);
+  w.blk = obase / (St::SPB * S);
+  w.own = w.blk * (St::SPB * S);
+  w.blk0 = __shfl_sync(0xffffffffu, w.blk, 0);
+  cx<C> ch[4][3];
+  stage_in<FT, S, A::SPB, St::SP>(chi, w.own, w.buf, w.ln);
+  __syncwarp();
+  load_spinor_sm<FT, S>(w.buf + (w.ln / S) * St::SP, w.lane, ch);
+  __syncwarp();
+  elem_t<FT> *o = out + (long long)plane * nplane + q;
+  const int ns = g.nsites;
+  force_prefetch<FT, S, PROJ, COMP12, 0>(psi, gauge, g, s, obase, w, w.buf);
+  cp_async_commit();
+  force_step<FT, S, PROJ, COMP12, 0>(psi, gauge, g, p, s, obase, w, ch, o, ns, active);
+  force_step<FT, S, PROJ, COMP12, 1>(psi, gauge, g, p, s, obase, w, ch, o, ns, active);
+  force_step<FT, S, PROJ, COMP12, 2>(psi, gauge, g, p, s, obase, w, ch, o, ns, active);
+  force_step<FT, S, PROJ, COMP12, 3>(psi, gauge, g, p, s, obase, w, ch, o, ns, active);
+  force_step<FT, S, PROJ, COMP12, 4>(psi, gauge, g, p, s, obase, w, ch, o, ns, active);
+  force_step<FT, S, PROJ, COMP12, 5>(psi, gauge, g, p, s, obase, w, ch, o, ns, active);
+  force_step<FT, S, PROJ, COMP12, 6>(psi, gauge, g, p, s, obase, w, ch, o, ns, active);
+  force_step<FT, S, PROJ, COMP12, 7>(psi, gauge, g, p, s, obase, w, ch, o, ns, active);
+}
+
+template <typename FT, int S>
+bool launch_async_s(bool proj, bool comp12, const elem_t<FT> *c, const elem_t<FT> *ps, const elem_t<FT> *u,
+                    elem_t<FT> *o, const GeoDev &g, const OpDev<comp_t<FT>> &p, cudaStream_t st)
+{
+  if constexpr (force_async_layout<FT, S>()) {
+    const long long warps = (long long)((g.nxh * g.ny + 31) / 32) * g.nz * g.nt;
+    const unsigned grid = (unsigned)((warps + 3) / 4);
+    if (!proj) async_force_kernel<FT, S, false, false><<<grid, 128, 0, st>>>(c, ps, u, o, g, p);
+    else if (comp12) async_force_kernel<FT, S, true, true><<<grid, 128, 0, st>>>(c, ps, u, o, g, p);
+    else async_force_kernel<FT, S, true, false><<<grid, 128, 0, st>>>(c, ps, u, o, g, p);
+    return true;
+  }
+  return false;
+}
+
 template <typename FT, int S>
 void launch_s(bool proj, bool comp12, int blocks, const elem_t<FT> *c, const elem_t<FT> *ps, const elem_t<FT> *u,
               elem_t<FT> *o, const GeoDev &g, const OpDev<comp_t<FT>> &p, cudaStream_t st)
@@ -194,6 +369,18 @@ cudaError_t launch_force(int S, bool proj, bool comp12, const void *chi, const v
   const int blocks = (g.nsites + 127) / 128;
   const E *c = (const E *)chi, *ps = (const E *)psi, *u = (const E *)gauge;
   E *o = (E *)out;
+  const bool aligned = ((uintptr_t)chi % 16 == 0) && ((uintptr_t)psi % 16 == 0) &&
+                       (!proj || (uintptr_t)gauge % 16 == 0);
+  if (g.V == S && aligned) {
+    bool done = false;
+    switch (S) {
+    case 4: done = launch_async_s<FT, 4>(proj, comp12, c, ps, u, o, g, p, st); break;
+    case 8: done = launch_async_s<FT, 8>(proj, comp12, c, ps, u, o, g, p, st); break;
+    case 16: done = launch_async_s<FT, 16>(proj, comp12, c, ps, u, o, g, p, st); break;
+    default: break;
+    }
+    if (done) return cudaGetLastError();
+  }
   switch (S) {
   case 1: launch_s<FT, 1>(proj, comp12, blocks, c, ps, u, o, g, p, st); break;
   case 2: launch_s<FT, 2>(proj, comp12, blocks, c, ps, u, o, g, p, st); break;

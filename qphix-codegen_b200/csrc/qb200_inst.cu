@@ -79,7 +79,9 @@ cudaError_t go(const KArgs<FT> &a, const GeoDev &g, const OpDev<typename ftraits
     const bool al = (((uintptr_t)a.psi | (uintptr_t)a.out | (uintptr_t)a.gauge) % 16 == 0) &&
                     (!ACH || (uintptr_t)a.chi % 16 == 0) && ((FAM != FAM_CLOVER && FAM != FAM_TMCLOV) || (uintptr_t)a.clov % 16 == 0);
     if (g.V == S && al) {
-      async_site_kernel<FT, S, COMP12, FAM, ACH><<<grid, kThreads, 0, st>>>(a, g, p);
+      const long long nb = warp_blocks(g);
+      if (nb > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+      async_site_kernel<FT, S, COMP12, FAM, ACH><<<(unsigned)nb, kThreads, 0, st>>>(a, g, p);
       return cudaGetLastError();
     }
   }
@@ -90,7 +92,9 @@ cudaError_t go(const KArgs<FT> &a, const GeoDev &g, const OpDev<typename ftraits
     const bool al = (((uintptr_t)a.psi | (uintptr_t)a.out | (uintptr_t)a.gauge) % 16 == 0) &&
                     (!ACH || (uintptr_t)a.chi % 16 == 0) && ((FAM != FAM_CLOVER && FAM != FAM_TMCLOV) || (uintptr_t)a.clov % 16 == 0);
     if (g.V == S && al) {
-      staged_site_kernel<FT, S, COMP12, FAM, ACH><<<grid, kThreads, 0, st>>>(a, g, p);
+      const long long nb = warp_blocks(g);
+      if (nb > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+      staged_site_kernel<FT, S, COMP12, FAM, ACH><<<(unsigned)nb, kThreads, 0, st>>>(a, g, p);
       return cudaGetLastError();
     }
   }

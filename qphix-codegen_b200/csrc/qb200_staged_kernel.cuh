@@ -386,17 +386,24 @@ __device__ __forceinline__ void staged_body(const KArgs<FT> &a, const GeoDev &g,
   __syncwarp();
 }
 
-// Grid as site_dslash_kernel (blockIdx.y = the (z, t) plane), blocks of 128
-// threads, at most 128 registers (4 blocks per SM).  Threads past the plane's
-// last site take part in the warp's copies (on a clamped site) and store
-// nothing.  Needs 16-byte aligned fields smaller than 32 GiB.
+// Work unit: one warp's 32 sites of one (z, t) plane, numbered over all
+// planes ((nxh*ny + 31)/32 per plane, so that no warp idles when a plane's
+// sites do not fill whole blocks); one-dimensional grid of blocks of 128
+// threads, at most 128 registers (4 blocks per SM).  Threads past the
+// plane's last site take part in the warp's copies (on a clamped site) and
+// store nothing.  Needs 16-byte aligned fields smaller than 32 GiB.
 template <typename FT, int S, bool COMP12, int FAM, bool ACH>
 __global__ void __launch_bounds__(128, 4)
     staged_site_kernel(const KArgs<FT> a, const GeoDev g, const OpDev<comp_t<FT>> p)
 {
   __shared__ __align__(16) unsigned char smem[4][StagedSmem<FT, S, COMP12>::BYTES];
-  staged_body<FT, S, COMP12, FAM, ACH>(a, g, p, blockIdx.y % g.nz, blockIdx.y / g.nz,
-                                       blockIdx.x * blockDim.x + threadIdx.x, smem[threadIdx.x >> 5]);
+  const int wpp = (g.nxh * g.ny + 31) >> 5;
+  const long long u = (long long)blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (u >= (long long)wpp * g.nz * g.nt) return; // whole warps
+  const int plane = (int)(u / wpp);
+  const int wi = (int)(u - (long long)plane * wpp);
+  staged_body<FT, S, COMP12, FAM, ACH>(a, g, p, plane % g.nz, plane / g.nz, wi * 32 + (threadIdx.x & 31),
+                                       smem[threadIdx.x >> 5]);
 }
 
 // Batched form: work unit = one warp's 32 sites of one plane of one item;
