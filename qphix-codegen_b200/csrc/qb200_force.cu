@@ -17,6 +17,7 @@
 // Re tr(X^dag P).  FP32 or FP64 storage, written in the storage type.
 // The reference has no backward kernels; this is an addition of the B200
 // build.
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <string>
@@ -206,19 +207,27 @@ __global__ void __launch_bounds__(128)
 // pieces per warp and component and wait one load latency per direction.
 // Here, as in async_site_kernel, a warp owns 32 sites of one (z, t) plane and
 // copies with cp.async, in 16-byte vectors, the blocks its sites need for
-// direction D+1 (the neighbour blocks, or its own blocks of psi for the x
-// directions, and with the projection the direction's link slab) into one of
-// two shared-memory buffers while it computes and stores the force of
-// direction D.  The arithmetic is force_from's; the output is written
-// directly (per component, a warp's stores are 32 consecutive sites).
+// direction D+1 (the neighbour blocks and, with the projection, the
+// direction's link slab) into one of two shared-memory buffers while it
+// computes and stores the force of direction D.  chi and an x region (the
+// warp's blocks, one on either side, the first block of its first row and
+// the last block of its last row: every x neighbour of its sites) are copied
+// with direction 0's link; the x region overlays spinor buffer 1, which
+// direction 3 is the first to use, and chi spinor buffer 0, read before
+// direction 2's copies go out.  The arithmetic is force_from's; the output is
+// written directly (per component, a warp's stores are 32 consecutive sites).
 template <typename FT, int S, bool PROJ, bool COMP12> struct ForceCfg {
   typedef Stage<FT, S> St;
   static constexpr int R = COMP12 ? 2 : 3;
   static constexpr int SPB = St::SPB * S * (int)sizeof(elem_t<FT>); // spinor block bytes
   static constexpr int LKB = R * 6 * S * (int)sizeof(elem_t<FT>);   // link slab bytes
   static constexpr int LKS = St::stride(R * 6);
-  static constexpr int HOP = St::G * (St::SP + (PROJ ? LKS : 0));
-  static constexpr int BUF = 2 * HOP;
+  static constexpr int XS = St::G + 4;                              // x region slots
+  static constexpr int S1 = St::G * St::SP;                         // spinor buffer 1 / x region
+  static constexpr int L0 = S1 + XS * St::SP;                       // link buffers
+  static constexpr int WB = L0 + (PROJ ? 2 * St::G * LKS : 0);      // bytes per warp
+  static constexpr int spin(int b) { return b ? S1 : 0; }
+  static constexpr int link(int b) { return L0 + b * St::G * LKS; }
 };
 
 template <typename FT, int S> constexpr bool force_async_layout()
@@ -226,19 +235,23 @@ template <typename FT, int S> constexpr bool force_async_layout()
   return (S == 4 || S == 8 || S == 16) && sizeof(elem_t<FT>) == 4;
 }
 
+// copies of direction D (D >= 2: the neighbour blocks; x directions read the
+// x region) and, projected, its link slab
 template <typename FT, int S, bool PROJ, bool COMP12, int D>
 __device__ __forceinline__ void force_prefetch(const elem_t<FT> *__restrict__ psi,
                                                const elem_t<FT> *__restrict__ gauge, const GeoDev &g, const Site &s,
-                                               long long obase, const WarpCtx &w, unsigned char *buf)
+                                               long long obase, const WarpCtx &w)
 {
   typedef ForceCfg<FT, S, PROJ, COMP12> A;
   typedef Stage<FT, S> St;
-  bool cross;
-  const long long nbase = obase + neighbour_offset<S, D>(g, s, (long long)St::SPB * S, 1, &cross);
-  stage_in_async<FT, S, A::SPB, St::SP>(psi, D < 2 ? w.own : nbase - w.lane, buf, w.ln);
+  if (D >= 2) {
+    bool cross;
+    const long long nbase = obase + neighbour_offset<S, D>(g, s, (long long)St::SPB * S, 1, &cross);
+    stage_in_async<FT, S, A::SPB, St::SP>(psi, nbase - w.lane, w.buf + A::spin(D & 1), w.ln);
+  }
   if (PROJ)
     stage_in_async<FT, S, A::LKB, A::LKS>(gauge, w.tile * (8LL * A::R * 6 * S) + (long long)D * A::R * 6 * S,
-                                          buf + St::G * St::SP, w.ln);
+                                          w.buf + A::link(D & 1), w.ln);
 }
 
 // one pipeline step: issue direction D+1, wait for D, read D's neighbour
@@ -253,30 +266,25 @@ __device__ __forceinline__ void force_step(const elem_t<FT> *__restrict__ psi, c
   typedef ForceCfg<FT, S, PROJ, COMP12> A;
   typedef Stage<FT, S> St;
   if (D < 7) {
-    force_prefetch<FT, S, PROJ, COMP12, (D < 7 ? D + 1 : 7)>(psi, gauge, g, s, obase, w,
-                                                             w.buf + ((D + 1) & 1) * A::HOP);
+    force_prefetch<FT, S, PROJ, COMP12, (D < 7 ? D + 1 : 7)>(psi, gauge, g, s, obase, w);
     cp_async_commit();
     cp_async_wait<1>();
   } else {
     cp_async_wait<0>();
   }
   __syncwarp();
-  const unsigned char *buf = w.buf + (D & 1) * A::HOP;
   cx<C> nb[4][3], G[3][3];
   if (D < 2) {
-    // the x neighbour: in the warp's own blocks of psi, else (a row end
-    // beyond the warp's blocks) read directly
-    bool cross;
-    const long long nbase = obase + neighbour_offset<S, D>(g, s, (long long)St::SPB * S, 1, &cross);
-    const long long nbk = nbase / (St::SPB * S);
-    const int nl = (int)(nbase - nbk * (St::SPB * S));
-    const long long gi = nbk - w.blk0;
-    if (gi >= 0 && gi < St::G) load_spinor_sm<FT, S>(buf + gi * St::SP, nl, nb);
-    else load_spinor<FT, S>(psi, nbase, nb);
+    int xb, nl;
+    x_neighbour<S, D>(g, s, xb, nl);
+    // slot of the row's first block, then of the neighbour's block
+    int sl = (int)(w.blk - w.blk0) + 1 - s.xcb / S + xb;
+    sl = (sl >= 0 && sl < St::G + 2) ? sl : (sl == w.xhead ? St::G + 2 : St::G + 3);
+    load_spinor_sm<FT, S>(w.xr + sl * St::SP, nl, nb);
   } else {
-    load_spinor_sm<FT, S>(buf + (w.ln / S) * St::SP, w.lane, nb);
+    load_spinor_sm<FT, S>(w.buf + A::spin(D & 1) + (w.ln / S) * St::SP, w.lane, nb);
   }
-  if (PROJ) load_link_sm<FT, S, COMP12>(buf + St::G * St::SP + (w.ln / S) * A::LKS, w.lane, G);
+  if (PROJ) load_link_sm<FT, S, COMP12>(w.buf + A::link(D & 1) + (w.ln / S) * A::LKS, w.lane, G);
   __syncwarp();
   if (active) force_from<FT, PROJ, D>(nb, chi, G, force_beta<C, D>(g, p, s), p, o, ns);
 }
@@ -284,8 +292,8 @@ __device__ __forceinline__ void force_step(const elem_t<FT> *__restrict__ psi, c
 // Work unit: one warp's 32 sites of one (z, t) plane, numbered over all
 // planes (wpp units per plane), so that no warp idles when a plane's sites
 // do not fill whole blocks; lanes past the plane's last site take part in
-// the copies (on a clamped site) and store nothing.  Fields 16-byte aligned,
-// below 32 GiB.
+// the copies (on a clamped site) and store nothing.  ForceCfg::WB bytes of
+// dynamic shared memory per warp; fields 16-byte aligned, below 32 GiB.
 template <typename FT, int S, bool PROJ, bool COMP12>
 __global__ void __launch_bounds__(128, 4)
     async_force_kernel(const elem_t<FT> *__restrict__ chi, const elem_t<FT> *__restrict__ psi,
@@ -295,7 +303,7 @@ __global__ void __launch_bounds__(128, 4)
   typedef comp_t<FT> C;
   typedef Stage<FT, S> St;
   typedef ForceCfg<FT, S, PROJ, COMP12> A;
-  __shared__ __align__(16) unsigned char smem[4][A::BUF];
+  extern __shared__ __align__(128) unsigned char fsmem[];
   const int nplane = g.nxh * g.ny;
   const int wpp = (nplane + 31) >> 5;
   const long long u = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -311,22 +319,28 @@ __global__ void __launch_bounds__(128, 4)
   s.xcb = q - s.y * g.nxh;
   s.par = (s.y + s.z + s.t + p.cb) & 1;
   WarpCtx w;
-  w.buf = smem[threadIdx.x >> 5];
+  w.buf = fsmem + (threadIdx.x >> 5) * A::WB;
   w.ln = threadIdx.x & 31;
   w.tile = tile_of<S>(g, s, &w.lane);
   const long long obase = spinor_base<FT, S>(g, s);
   w.blk = obase / (St::SPB * S);
   w.own = w.blk * (St::SPB * S);
   w.blk0 = __shfl_sync(0xffffffffu, w.blk, 0);
-  cx<C> ch[4][3];
-  stage_in<FT, S, A::SPB, St::SP>(chi, w.own, w.buf, w.ln);
+  w.xr = w.buf + A::S1;
+  w.xhead = 1 - __shfl_sync(0xffffffffu, s.xcb, 0) / S;
+  const long long tail = __shfl_sync(0xffffffffu, w.blk, 31) - __shfl_sync(0xffffffffu, s.xcb, 31) / S + g.nvecs - 1;
+  // chi, the x region and direction 0's link in one group
+  stage_in_async<FT, S, A::SPB, St::SP>(chi, w.own, w.buf, w.ln);
+  stage_xregion<FT, S, COMP12>(psi, w.blk0, w.blk0 - 1 + w.xhead, tail, g.Pxyz * g.nt, w.xr, w.ln);
+  force_prefetch<FT, S, PROJ, COMP12, 0>(psi, gauge, g, s, obase, w);
+  cp_async_commit();
+  cp_async_wait<0>();
   __syncwarp();
+  cx<C> ch[4][3];
   load_spinor_sm<FT, S>(w.buf + (w.ln / S) * St::SP, w.lane, ch);
   __syncwarp();
   elem_t<FT> *o = out + (long long)plane * nplane + q;
   const int ns = g.nsites;
-  force_prefetch<FT, S, PROJ, COMP12, 0>(psi, gauge, g, s, obase, w, w.buf);
-  cp_async_commit();
   force_step<FT, S, PROJ, COMP12, 0>(psi, gauge, g, p, s, obase, w, ch, o, ns, active);
   force_step<FT, S, PROJ, COMP12, 1>(psi, gauge, g, p, s, obase, w, ch, o, ns, active);
   force_step<FT, S, PROJ, COMP12, 2>(psi, gauge, g, p, s, obase, w, ch, o, ns, active);
@@ -337,16 +351,39 @@ __global__ void __launch_bounds__(128, 4)
   force_step<FT, S, PROJ, COMP12, 7>(psi, gauge, g, p, s, obase, w, ch, o, ns, active);
 }
 
+template <typename FT, int S, bool PROJ, bool COMP12>
+cudaError_t go_async_force(const elem_t<FT> *c, const elem_t<FT> *ps, const elem_t<FT> *u, elem_t<FT> *o,
+                           const GeoDev &g, const OpDev<comp_t<FT>> &p, cudaStream_t st)
+{
+  typedef ForceCfg<FT, S, PROJ, COMP12> A;
+  const long long warps = (long long)((g.nxh * g.ny + 31) / 32) * g.nz * g.nt;
+  const long long blocks = (warps + 3) / 4;
+  if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+  const int smem = 4 * A::WB;
+  // the dynamic shared-memory limit of this kernel, raised once per device
+  static std::atomic<unsigned long long> raised{0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!(raised.load() & (1ull << dev))) {
+    e = cudaFuncSetAttribute(async_force_kernel<FT, S, PROJ, COMP12>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             smem);
+    if (e != cudaSuccess) return e;
+    raised.fetch_or(1ull << dev);
+  }
+  async_force_kernel<FT, S, PROJ, COMP12><<<(unsigned)blocks, 128, smem, st>>>(c, ps, u, o, g, p);
+  return cudaGetLastError();
+}
+
 template <typename FT, int S>
 bool launch_async_s(bool proj, bool comp12, const elem_t<FT> *c, const elem_t<FT> *ps, const elem_t<FT> *u,
-                    elem_t<FT> *o, const GeoDev &g, const OpDev<comp_t<FT>> &p, cudaStream_t st)
+                    elem_t<FT> *o, const GeoDev &g, const OpDev<comp_t<FT>> &p, cudaStream_t st, cudaError_t *e)
 {
   if constexpr (force_async_layout<FT, S>()) {
-    const long long warps = (long long)((g.nxh * g.ny + 31) / 32) * g.nz * g.nt;
-    const unsigned grid = (unsigned)((warps + 3) / 4);
-    if (!proj) async_force_kernel<FT, S, false, false><<<grid, 128, 0, st>>>(c, ps, u, o, g, p);
-    else if (comp12) async_force_kernel<FT, S, true, true><<<grid, 128, 0, st>>>(c, ps, u, o, g, p);
-    else async_force_kernel<FT, S, true, false><<<grid, 128, 0, st>>>(c, ps, u, o, g, p);
+    if (!proj) *e = go_async_force<FT, S, false, false>(c, ps, u, o, g, p, st);
+    else if (comp12) *e = go_async_force<FT, S, true, true>(c, ps, u, o, g, p, st);
+    else *e = go_async_force<FT, S, true, false>(c, ps, u, o, g, p, st);
     return true;
   }
   return false;
@@ -373,13 +410,14 @@ cudaError_t launch_force(int S, bool proj, bool comp12, const void *chi, const v
                        (!proj || (uintptr_t)gauge % 16 == 0);
   if (g.V == S && aligned) {
     bool done = false;
+    cudaError_t e = cudaSuccess;
     switch (S) {
-    case 4: done = launch_async_s<FT, 4>(proj, comp12, c, ps, u, o, g, p, st); break;
-    case 8: done = launch_async_s<FT, 8>(proj, comp12, c, ps, u, o, g, p, st); break;
-    case 16: done = launch_async_s<FT, 16>(proj, comp12, c, ps, u, o, g, p, st); break;
+    case 4: done = launch_async_s<FT, 4>(proj, comp12, c, ps, u, o, g, p, st, &e); break;
+    case 8: done = launch_async_s<FT, 8>(proj, comp12, c, ps, u, o, g, p, st, &e); break;
+    case 16: done = launch_async_s<FT, 16>(proj, comp12, c, ps, u, o, g, p, st, &e); break;
     default: break;
     }
-    if (done) return cudaGetLastError();
+    if (done) return e;
   }
   switch (S) {
   case 1: launch_s<FT, 1>(proj, comp12, blocks, c, ps, u, o, g, p, st); break;
