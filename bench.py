@@ -47,7 +47,9 @@ def parse():
     ap.add_argument("--soalen", type=int, default=16)
     ap.add_argument("--veclen", type=int, default=0)
     ap.add_argument("--dims", default="32,32,32,64")
-    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=40,
+                    help="steps of the end-to-end pipeline; its drain (one kernel and one device-to-host "
+                         "copy) is amortised over them")
     ap.add_argument("--nrhs", type=int, default=8, help="right-hand sides of --only solve_tm_mrhs")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bound of the CPU baseline sample")
@@ -459,6 +461,26 @@ def bench_solve_tm_mrhs(dev, dims=(48, 48, 48, 96), kappa=0.16, mu=0.01, nrhs=8)
           for i in range(nrhs)]
     out = {"lattice": list(dims), "family": "tm", "kappa": kappa, "mu": mu, "tol": 1e-10, "nrhs": nrhs,
            "soalen": 8, "inner_storage": "fp16 multi-RHS (links fp16, 12-real)"}
+    # the FP16 multi-RHS operator's two kernels on this lattice: the plain
+    # twisted-mass dslash (other checkerboard) and the A.chi - b.D.psi form;
+    # bytes per right-hand-side site: psi + out (+ chi) 48 each + 12-real
+    # FP16 links 192 / nrhs
+    g16 = G.with_(ftype=F16)
+    stream = torch.cuda.current_stream()
+    peak = measured_peak()[0]
+    op16 = ops_[F16]
+    mp = torch.randn(g16.spinor_elems * nrhs, device=dev).half()
+    mc = torch.randn(g16.spinor_elems * nrhs, device=dev).half()
+    mo = torch.zeros_like(mp)
+    kw = dict(coeff_s=0.5, coeff_t_f=0.5, coeff_t_b=0.5, mu=mu / alpha, muinv=alpha / (alpha ** 2 + mu ** 2))
+    n_rs = g16.vol_cb * nrhs
+    for kern, extra, bps in (("dslash", {}, 96 + 192 / nrhs),
+                             ("achimbdpsi", {"chi": mc, "alpha": alpha}, 144 + 192 / nrhs)):
+        ms = _time(lambda: mrhs.dslash(g16, nrhs, "tm", kern, 1, 0, mp, mo, op16.keep[0][0], **extra, **kw), 20, stream)
+        out["mrhs_tm_%s" % kern] = {"ms": ms, "gbs": bps * n_rs / (ms * 1e-3) / 1e9,
+                                    "frac_of_peak": bps * n_rs / (ms * 1e-3) / 1e9 / peak,
+                                    "bytes_per_rhs_site": bps}
+    del mp, mc, mo
     mixed_solve(ops_[F64], ops_[F32], bs[0], tol=1e-4, inner_tol=1e-2)
     mrhs.mixed_solve(ops_[F64], ops_[F16], bs, tol=1e-3, inner_tol=1e-2, solver="cg_reliable")
 

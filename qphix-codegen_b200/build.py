@@ -66,8 +66,27 @@ def newest_header():
                for d in (CSRC, INCLUDE) for f in os.listdir(d) if not f.endswith(".cu"))
 
 
+def deps_of(obj, extra, src):
+    """Files the unit was compiled from, read from the dependency file nvcc
+    wrote beside the object.  An object built without one is checked against
+    every header of csrc/ and include/; when it is newer than all of them its
+    dependency file is written now (nvcc -M, preprocessing only)."""
+    dfile = obj + ".d"
+    if not os.path.exists(dfile) and os.path.getmtime(obj) >= max(newest_header(), os.path.getmtime(src)):
+        subprocess.run([nvcc()] + ARCH + NVFLAGS + extra + ["-M", "-MT", obj, "-MF", dfile, src],
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    if os.path.exists(dfile):
+        with open(dfile) as f:
+            text = f.read().replace("\\\n", " ")
+        _, _, rhs = text.partition(":")
+        files = [p for p in rhs.split() if os.path.exists(p)]
+        if files:
+            return files
+    return [src] + [os.path.join(d, f) for d in (CSRC, INCLUDE) for f in os.listdir(d) if not f.endswith(".cu")]
+
+
 def compile_one(obj, extra, src, log):
-    cmd = [nvcc()] + ARCH + NVFLAGS + extra + ["-c", src, "-o", obj]
+    cmd = [nvcc()] + ARCH + NVFLAGS + extra + ["-MD", "-MF", obj + ".d", "-c", src, "-o", obj]
     r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
     with open(log, "w") as f:
         f.write(" ".join(cmd) + "\n" + r.stdout)
@@ -84,10 +103,10 @@ def build(jobs=None, force=False, verbose=True):
         return LIB
     jobs = jobs or max(1, os.cpu_count() or 1)
     todo = []
-    hdr_t = newest_header()
     for obj, extra, src in units():
-        # a unit depends on its own source and on every header
-        dep_t = max(hdr_t, os.path.getmtime(src))
+        # a unit depends on its source and the headers it included
+        if not force and os.path.exists(obj):
+            dep_t = max(os.path.getmtime(p) for p in deps_of(obj, extra, src))
         if force or not os.path.exists(obj) or os.path.getmtime(obj) < dep_t:
             todo.append((obj, extra, src, obj + ".log"))
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:

@@ -23,6 +23,10 @@
 //     costs a few instructions.  (cp.async.bulk from one lane per piece was
 //     tried: its operands must be warp-uniform, and with a piece per group
 //     the compiler serialises the copies at 10-20 instructions each.)
+//   * for SOALEN 8 and 16 the y/z/t neighbour blocks, the link slabs and chi
+//     are read from shared memory with ldmatrix, four elements of the
+//     thread's two lanes per instruction (tw_ld_elems), a quarter of the
+//     32-bit shared loads;
 //   * the x neighbours come from an x region staged once (the warp's blocks,
 //     one on either side, the first block of the first row and the last
 //     block of the last row), which overlays the second spinor buffer; the
@@ -111,6 +115,49 @@ template <typename FT, int S>
 __device__ __forceinline__ float2 tw_ld2(const unsigned char *grp, int k, int l)
 {
   return tw_io<FT>::cv2(reinterpret_cast<const elem_t<FT> *>(grp) + k * S + l);
+}
+
+// two adjacent stored elements held in a 32-bit register -> float2
+template <typename FT> __device__ __forceinline__ float2 tw_cvt(unsigned v)
+{
+  return tw_io<FT>::cv2(&v);
+}
+
+__device__ __forceinline__ void ldsm_x4(unsigned addr, unsigned &r0, unsigned &r1, unsigned &r2, unsigned &r3)
+{
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];\n"
+               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+               : "r"(addr));
+}
+__device__ __forceinline__ void ldsm_x2(unsigned addr, unsigned &r0, unsigned &r1)
+{
+  asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0, %1}, [%2];\n" : "=r"(r0), "=r"(r1) : "r"(addr));
+}
+
+// Elements 0..NE-1 of the thread's lanes (2 tig, 2 tig + 1) in its group's
+// staged piece (group r's piece at base + r * GST, element k at + k * 2S
+// bytes), as raw 32-bit pairs.  S = 8, 16: ldmatrix, four elements per
+// instruction -- matrix m of pass q is element 4q + m of the warp's groups,
+// one 16-byte row per group (two for S = 16), and thread t receives bytes
+// 4 (t % 4) of row t / 4, which are its own two lanes.  S = 4 (an element
+// of a group is 8 bytes, half a row): 32-bit loads.  All 32 lanes call it.
+template <typename FT, int S, int GST, int NE>
+__device__ __forceinline__ void tw_ld_elems(const unsigned char *base, int ln, unsigned (&v)[NE])
+{
+  static_assert(NE % 2 == 0, "elements in pairs");
+  if constexpr (S >= 8) {
+    static_assert(GST % 16 == 0, "16-byte aligned rows");
+    constexpr int RPG = S / 8; // 16-byte rows per element of a group
+    const int r = ln & 7, m = ln >> 3;
+    const unsigned a = (unsigned)__cvta_generic_to_shared(base) + (unsigned)((r / RPG) * GST + m * 2 * S + (r % RPG) * 16);
+#pragma unroll
+    for (int q = 0; q < NE / 4; q++) ldsm_x4(a + q * 8 * S, v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+    if constexpr (NE % 4 == 2) ldsm_x2(a + (NE / 4) * 8 * S, v[NE - 2], v[NE - 1]);
+  } else {
+    const int gi = ln / (S / 2), tig = ln - gi * (S / 2);
+#pragma unroll
+    for (int k = 0; k < NE; k++) v[k] = *reinterpret_cast<const unsigned *>(base + gi * GST + k * 2 * S + 4 * tig);
+  }
 }
 
 __device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
@@ -394,12 +441,14 @@ __device__ __forceinline__ void tw_compute_hop(const GeoDev &g, const OpDev<floa
                         reinterpret_cast<const float *>(gb + 48 * S)[lb]);
   } else {
     const unsigned char *grp = w.buf + (D & 1) * T::X0 + w.gi * T::SP;
+    unsigned v[24];
+    tw_ld_elems<FT, S, T::SP, 24>(w.buf + (D & 1) * T::X0, w.ln, v);
 #pragma unroll
     for (int c = 0; c < 3; c++)
 #pragma unroll
       for (int sp = 0; sp < 4; sp++) {
-        psi[sp][c].re = tw_ld2<FT, S>(grp, (c * 4 + sp) * 2 + 0, w.lane);
-        psi[sp][c].im = tw_ld2<FT, S>(grp, (c * 4 + sp) * 2 + 1, w.lane);
+        psi[sp][c].re = tw_cvt<FT>(v[(c * 4 + sp) * 2 + 0]);
+        psi[sp][c].im = tw_cvt<FT>(v[(c * 4 + sp) * 2 + 1]);
       }
     if (T::SPB == 26) nrm = reinterpret_cast<const float2 *>(grp + 48 * S)[w.lane >> 1];
     bool cross;
@@ -408,13 +457,14 @@ __device__ __forceinline__ void tw_compute_hop(const GeoDev &g, const OpDev<floa
   }
   c2 G[3][3];
   {
-    const unsigned char *lg = w.buf + T::LOFF + ((D & 1) * T::G + w.gi) * T::LKS;
+    unsigned v[T::R * 6];
+    tw_ld_elems<FT, S, T::LKS, T::R * 6>(w.buf + T::LOFF + (D & 1) * T::G * T::LKS, w.ln, v);
 #pragma unroll
     for (int r = 0; r < T::R; r++)
 #pragma unroll
       for (int c = 0; c < 3; c++) {
-        G[r][c].re = tw_ld2<FT, S>(lg, (r * 3 + c) * 2 + 0, w.lane);
-        G[r][c].im = tw_ld2<FT, S>(lg, (r * 3 + c) * 2 + 1, w.lane);
+        G[r][c].re = tw_cvt<FT>(v[(r * 3 + c) * 2 + 0]);
+        G[r][c].im = tw_cvt<FT>(v[(r * 3 + c) * 2 + 1]);
       }
     if (COMP12) recon_row3_2(G);
   }
@@ -554,12 +604,14 @@ __device__ __forceinline__ void twin_body(const KArgs<FT> &a, const GeoDev &g, c
       const unsigned char *grp = w.buf + w.gi * T::SP;
       float2 cn = make_float2(1.f, 1.f);
       if (T::SPB == 26) cn = reinterpret_cast<const float2 *>(grp + 48 * S)[w.lane >> 1];
+      unsigned v[24];
+      tw_ld_elems<FT, S, T::SP, 24>(w.buf, w.ln, v);
 #pragma unroll
       for (int c = 0; c < 3; c++)
 #pragma unroll
         for (int sp = 0; sp < 4; sp++) {
-          ch[sp][c].re = tw_ld2<FT, S>(grp, (c * 4 + sp) * 2 + 0, w.lane);
-          ch[sp][c].im = tw_ld2<FT, S>(grp, (c * 4 + sp) * 2 + 1, w.lane);
+          ch[sp][c].re = tw_cvt<FT>(v[(c * 4 + sp) * 2 + 0]);
+          ch[sp][c].im = tw_cvt<FT>(v[(c * 4 + sp) * 2 + 1]);
           if (T::SPB == 26) {
             ch[sp][c].re = f2mul(ch[sp][c].re, cn);
             ch[sp][c].im = f2mul(ch[sp][c].im, cn);
