@@ -8,6 +8,10 @@
 // own blocks of psi for the x hops, and the direction-(D+1) slab of its link
 // tiles) into one of two shared-memory buffers while it computes hop D from
 // the other, so the copies cost no registers and overlap the arithmetic.
+// The post-hop term's operands follow the same way: chi (or the first
+// CloverBlock half of the clover dslash) is copied into hop buffer 0 while
+// hop 7 computes, and each further CloverBlock half into a freed hop buffer
+// while the previous one computes.
 // The per-site reads from shared memory, the x-neighbour handling and the
 // clover / chi / result staging are those of qb200_staged_kernel.cuh; the
 // arithmetic is that of site_body, operation for operation.
@@ -174,15 +178,39 @@ __device__ __forceinline__ void compute_hop(const KArgs<FT> &a, const GeoDev &g,
   recons<C, MU>(ub, beta, tau, acc);
 }
 
-// one pipeline step: issue hop D+1, wait for hop D, compute hop D
-template <typename FT, int S, bool COMP12, int D>
+// The first operand of the post-hop term, copied into hop buffer 0 while hop
+// 7 computes from buffer 1: chi for the A.chi - b.D.psi forms, else the
+// first CloverBlock half of the clover dslash (none for the other forms).
+template <typename FT, int FAM, bool ACH> struct AsyncTail {
+  static constexpr bool CHI = ACH;
+  static constexpr bool CLOVER0 = !ACH && FAM == FAM_CLOVER;
+  static constexpr bool ANY = CHI || CLOVER0;
+};
+
+template <typename FT, int S, bool COMP12, int FAM, bool ACH>
+__device__ __forceinline__ void prefetch_tail(const KArgs<FT> &a, const WarpCtx &w)
+{
+  typedef Stage<FT, S> St;
+  typedef AsyncTail<FT, FAM, ACH> TL;
+  if constexpr (TL::CHI) stage_in_async<FT, S, AsyncCfg<FT, S, COMP12>::SPB, St::SP>(a.chi, w.own, w.buf, w.ln);
+  if constexpr (TL::CLOVER0)
+    stage_in_async<FT, S, 36 * S * (int)sizeof(elem_t<FT>), St::CL>(a.clov, w.tile * (72LL * S), w.buf, w.ln);
+}
+
+// one pipeline step: issue hop D+1 (after hop 6: the post-hop term's first
+// operand, prefetch_tail), wait for hop D, compute hop D
+template <typename FT, int S, bool COMP12, int FAM, bool ACH, int D>
 __device__ __forceinline__ void pipe_step(const KArgs<FT> &a, const GeoDev &g, const OpDev<comp_t<FT>> &p,
                                           const Site &s, long long obase, const WarpCtx &w,
                                           cx<comp_t<FT>> (&acc)[4][3])
 {
   typedef AsyncCfg<FT, S, COMP12> A;
-  if (D < 7) {
-    prefetch_hop<FT, S, COMP12, (D < 7 ? D + 1 : 7)>(a, g, s, obase, w, w.buf + ((D + 1) & 1) * A::HOP);
+  if constexpr (D < 7) {
+    prefetch_hop<FT, S, COMP12, D + 1>(a, g, s, obase, w, w.buf + ((D + 1) & 1) * A::HOP);
+    cp_async_commit();
+    cp_async_wait<1>();
+  } else if constexpr (AsyncTail<FT, FAM, ACH>::ANY) {
+    prefetch_tail<FT, S, COMP12, FAM, ACH>(a, w); // hop buffer 0 is free: hop 6 was the last to read it
     cp_async_commit();
     cp_async_wait<1>();
   } else {
@@ -193,21 +221,51 @@ __device__ __forceinline__ void pipe_step(const KArgs<FT> &a, const GeoDev &g, c
   __syncwarp();
 }
 
-template <typename FT, int S, bool COMP12>
+template <typename FT, int S, bool COMP12, int FAM, bool ACH>
 __device__ __forceinline__ void async_hops(const KArgs<FT> &a, const GeoDev &g, const OpDev<comp_t<FT>> &p,
                                            const Site &s, long long obase, const WarpCtx &w,
                                            cx<comp_t<FT>> (&acc)[4][3])
 {
   prefetch_hop<FT, S, COMP12, 0>(a, g, s, obase, w, w.buf);
   cp_async_commit();
-  pipe_step<FT, S, COMP12, 0>(a, g, p, s, obase, w, acc);
-  pipe_step<FT, S, COMP12, 1>(a, g, p, s, obase, w, acc);
-  pipe_step<FT, S, COMP12, 2>(a, g, p, s, obase, w, acc);
-  pipe_step<FT, S, COMP12, 3>(a, g, p, s, obase, w, acc);
-  pipe_step<FT, S, COMP12, 4>(a, g, p, s, obase, w, acc);
-  pipe_step<FT, S, COMP12, 5>(a, g, p, s, obase, w, acc);
-  pipe_step<FT, S, COMP12, 6>(a, g, p, s, obase, w, acc);
-  pipe_step<FT, S, COMP12, 7>(a, g, p, s, obase, w, acc);
+  pipe_step<FT, S, COMP12, FAM, ACH, 0>(a, g, p, s, obase, w, acc);
+  pipe_step<FT, S, COMP12, FAM, ACH, 1>(a, g, p, s, obase, w, acc);
+  pipe_step<FT, S, COMP12, FAM, ACH, 2>(a, g, p, s, obase, w, acc);
+  pipe_step<FT, S, COMP12, FAM, ACH, 3>(a, g, p, s, obase, w, acc);
+  pipe_step<FT, S, COMP12, FAM, ACH, 4>(a, g, p, s, obase, w, acc);
+  pipe_step<FT, S, COMP12, FAM, ACH, 5>(a, g, p, s, obase, w, acc);
+  pipe_step<FT, S, COMP12, FAM, ACH, 6>(a, g, p, s, obase, w, acc);
+  pipe_step<FT, S, COMP12, FAM, ACH, 7>(a, g, p, s, obase, w, acc);
+}
+
+// The CloverBlock (both halves) applied to in, MODE into out: half 0 is in
+// hop buffer 0 (prefetch_tail's copy, or `issue0` copies it now), half 1 is
+// copied into hop buffer 1 here, so that it lands while half 0 computes.
+// The operations of staged_clover.
+template <typename FT, int S, bool COMP12, int MODE, bool RHO>
+__device__ __forceinline__ void async_clover(const KArgs<FT> &a, const WarpCtx &w, int isPlus, comp_t<FT> rho,
+                                             bool issue0, const cx<comp_t<FT>> (&in)[4][3],
+                                             cx<comp_t<FT>> (&out)[4][3])
+{
+  typedef Stage<FT, S> St;
+  typedef AsyncCfg<FT, S, COMP12> A;
+  constexpr int CLB = 36 * S * (int)sizeof(elem_t<FT>);
+  static_assert(St::G * St::CL <= A::HOP, "a CloverBlock half fits in a hop buffer");
+  if (issue0) {
+    stage_in_async<FT, S, CLB, St::CL>(a.clov, w.tile * (72LL * S), w.buf, w.ln);
+    cp_async_commit();
+  }
+  stage_in_async<FT, S, CLB, St::CL>(a.clov, w.tile * (72LL * S) + 36LL * S, w.buf + A::HOP, w.ln);
+  cp_async_commit();
+  cp_async_wait<1>();
+  __syncwarp();
+  clover_block_sm<FT, S, MODE, RHO>(w.buf + (w.ln / S) * St::CL, w.lane, 0,
+                                    rho_of_block<comp_t<FT>>(0, isPlus, rho), in, out);
+  cp_async_wait<0>();
+  __syncwarp();
+  clover_block_sm<FT, S, MODE, RHO>(w.buf + A::HOP + (w.ln / S) * St::CL, w.lane, 1,
+                                    rho_of_block<comp_t<FT>>(1, isPlus, rho), in, out);
+  __syncwarp();
 }
 
 // The operator at site q0 (this lane's) of plane (z, t), all 32 lanes of a
@@ -249,24 +307,46 @@ __device__ __forceinline__ void async_body(const KArgs<FT> &a, const GeoDev &g, 
   for (int sp = 0; sp < 4; sp++)
 #pragma unroll
     for (int c = 0; c < 3; c++) acc[sp][c] = mk<C>(0, 0);
-  async_hops<FT, S, COMP12>(a, g, p, s, obase, w, acc);
+  async_hops<FT, S, COMP12, FAM, ACH>(a, g, p, s, obase, w, acc);
   cx<C> res[4][3];
   if (ACH) {
-    // the hops (subtracted: beta negated by the host), then + A.chi
+    // the hops (subtracted: beta negated by the host), then + A.chi; chi is
+    // in hop buffer 0 (copied during hop 7)
     cx<C> ch[4][3];
-    stage_in<FT, S, A::SPB, St::SP>(a.chi, w.own, w.buf, w.ln);
+    if (FAM == FAM_CLOVER) {
+      // CloverBlock half 0 into hop buffer 1 while chi is read out
+      stage_in_async<FT, S, 36 * S * (int)sizeof(elem_t<FT>), St::CL>(a.clov, w.tile * (72LL * S),
+                                                                        w.buf + A::HOP, w.ln);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
     __syncwarp();
     load_spinor_sm<FT, S>(w.buf + (w.ln / S) * St::SP, w.lane, ch);
     __syncwarp();
-    if (FAM == FAM_CLOVER) staged_clover<FT, S, MODE_ADD, true>(a, w, p.isPlus, p.rho, ch, acc);
-    else if (FAM == FAM_TMCLOV) staged_full_clover<FT, S, MODE_ADD, true>(a, w, p.isPlus, p.rho, ch, acc);
+    if (FAM == FAM_CLOVER) {
+      // half 1 into hop buffer 0 (chi is in registers), then both halves
+      constexpr int CLB = 36 * S * (int)sizeof(elem_t<FT>);
+      stage_in_async<FT, S, CLB, St::CL>(a.clov, w.tile * (72LL * S) + 36LL * S, w.buf, w.ln);
+      cp_async_commit();
+      cp_async_wait<1>();
+      __syncwarp();
+      clover_block_sm<FT, S, MODE_ADD, true>(w.buf + A::HOP + (w.ln / S) * St::CL, w.lane, 0,
+                                             rho_of_block<C>(0, p.isPlus, p.rho), ch, acc);
+      cp_async_wait<0>();
+      __syncwarp();
+      clover_block_sm<FT, S, MODE_ADD, true>(w.buf + (w.ln / S) * St::CL, w.lane, 1,
+                                             rho_of_block<C>(1, p.isPlus, p.rho), ch, acc);
+      __syncwarp();
+    } else if (FAM == FAM_TMCLOV) staged_full_clover<FT, S, MODE_ADD, true>(a, w, p.isPlus, p.rho, ch, acc);
     else ach_finish<FT, FAM>(a, p, w.tile, w.lane, S, ch, acc);
 #pragma unroll
     for (int sp = 0; sp < 4; sp++)
 #pragma unroll
       for (int c = 0; c < 3; c++) res[sp][c] = acc[sp][c];
   } else {
-    if (FAM == FAM_CLOVER) staged_clover<FT, S, MODE_SET, false>(a, w, p.isPlus, (C)0, acc, res);
+    if (FAM == FAM_CLOVER) async_clover<FT, S, COMP12, MODE_SET, false>(a, w, p.isPlus, (C)0, false, acc, res);
     else if (FAM == FAM_TMCLOV) staged_full_clover<FT, S, MODE_SET, false>(a, w, p.isPlus, (C)0, acc, res);
     else plain_post<FT, FAM>(a, p, w.tile, w.lane, S, acc, res);
   }
