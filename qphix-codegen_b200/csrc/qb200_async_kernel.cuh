@@ -369,8 +369,20 @@ __host__ __device__ __forceinline__ long long warp_units(const GeoDev &g)
 }
 inline long long warp_blocks(const GeoDev &g) { return (warp_units(g) + 3) / 4; }
 
+// resident blocks per SM the register allocation must allow: five for the
+// 32-bit clover forms (their 38.9 KB of shared memory per block fit five
+// times; the others already stay under 102 registers or hold more shared
+// memory), four otherwise
+#ifndef QB_ASYNC_MINB_CLOVER
+#define QB_ASYNC_MINB_CLOVER 5
+#endif
+template <typename FT, int FAM> constexpr int async_minb()
+{
+  return (FAM == FAM_CLOVER && sizeof(elem_t<FT>) == 4) ? QB_ASYNC_MINB_CLOVER : 4;
+}
+
 template <typename FT, int S, bool COMP12, int FAM, bool ACH>
-__global__ void __launch_bounds__(128, 4)
+__global__ void __launch_bounds__(128, async_minb<FT, FAM>())
     async_site_kernel(const KArgs<FT> a, const GeoDev g, const OpDev<comp_t<FT>> p)
 {
   __shared__ __align__(16) unsigned char smem[4][AsyncCfg<FT, S, COMP12>::BUF];
