@@ -283,18 +283,22 @@ __device__ __forceinline__ void herm_apply_tw(const unsigned char *grp, int l, i
   }
 }
 
-// dense_apply on a pair of sites from a staged FullCloverBlock half
+// dense_apply (a dense FullCloverBlock half on a pair of sites) for rows r0,
+// r0 + 1 of block `blk` only, their 24 elements staged at grp (element
+// (r - r0) * 12 + 2c + ri); dense_apply's operations per row, so the block
+// applied two rows at a time gives the same bits
 template <typename FT, int S, int MODE, bool RHO>
-__device__ __forceinline__ void dense_apply_tw(const unsigned char *grp, int l, int blk, float rhob,
-                                               const c2 (&in)[4][3], c2 (&out)[4][3])
+__device__ __forceinline__ void dense_rows_tw(const unsigned char *grp, int l, int blk, int r0, float rhob,
+                                              const c2 (&in)[4][3], c2 (&out)[4][3])
 {
 #pragma unroll
-  for (int r = 0; r < 6; r++) {
+  for (int rr = 0; rr < 2; rr++) {
+    const int r = r0 + rr;
     float2 re1 = bc(0.f), im1 = bc(0.f), re2 = bc(0.f), im2 = bc(0.f);
 #pragma unroll
     for (int c = 0; c < 6; c++) {
-      const float2 ar = tw_ld2<FT, S>(grp, (r * 6 + c) * 2 + 0, l);
-      const float2 ai = tw_ld2<FT, S>(grp, (r * 6 + c) * 2 + 1, l);
+      const float2 ar = tw_ld2<FT, S>(grp, (rr * 6 + c) * 2 + 0, l);
+      const float2 ai = tw_ld2<FT, S>(grp, (rr * 6 + c) * 2 + 1, l);
       const c2 w = in[2 * blk + c / 3][c % 3];
       if (c < 3) {
         re1 = f2fma(ar, w.re, re1);
@@ -485,15 +489,70 @@ __device__ __forceinline__ void tw_compute_hop(const GeoDev &g, const OpDev<floa
   recons2v<MU>(ub, b2, ((p.isPlus != 0) != FWD) ? 1.f : -1.f, acc);
 }
 
+// the group's FullCloverBlock of its tile (tl), taken two rows of a half at a
+// time: piece q (0..5) is rows 2 (q % 3), 2 (q % 3) + 1 of half q / 3, 24
+// consecutive elements per lane; it goes into spinor buffer b's slot of the
+// group (24 elements fit in a spinor block's slot)
+template <typename FT, int S, bool COMP12>
+__device__ __forceinline__ void tw_issue_fcl_piece(const KArgs<FT> &a, const TwinCtx &w, long long tl, int q, int b)
+{
+  typedef TwinCfg<FT, S, COMP12> T;
+  static_assert(24 <= T::SPB, "a piece fits in a spinor slot");
+  tw_cp<24 * S * 2, T::TPG>(w.buf + (b ? T::X0 : 0) + w.gi * T::SP,
+                            a.clov + tl * (144LL * S) + (q / 3) * 72LL * S + (q % 3) * 24LL * S, w.tig);
+}
+
+// the pair's tile, from the table written at the start
+template <typename FT, int S, bool COMP12> __device__ __forceinline__ long long tw_tile(const TwinCtx &w)
+{
+  typedef TwinCfg<FT, S, COMP12> T;
+  return reinterpret_cast<const long long *>(w.buf + T::DOFF + 6 * 32 * 4)[w.ln];
+}
+
+// The FullCloverBlock applied to in (MODE into out) in its six pieces, piece
+// q read from spinor buffer (q + B0) & 1; piece 0's copy is in flight on
+// entry, and each further piece is copied while the one before computes.
+template <typename FT, int S, bool COMP12, int MODE, bool RHO, int B0>
+__device__ __forceinline__ void tw_full_clover_pieces(const KArgs<FT> &a, const TwinCtx &w, long long tl, int isPlus,
+                                                      float rho, const c2 (&in)[4][3], c2 (&out)[4][3])
+{
+  typedef TwinCfg<FT, S, COMP12> T;
+#pragma unroll
+  for (int q = 0; q < 6; q++) {
+    if (q < 5) {
+      tw_issue_fcl_piece<FT, S, COMP12>(a, w, tl, q + 1, (q + 1 + B0) & 1);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncwarp();
+    dense_rows_tw<FT, S, MODE, RHO>(w.buf + (((q + B0) & 1) ? T::X0 : 0) + w.gi * T::SP, w.lane, q / 3, 2 * (q % 3),
+                                    rho_of_block<float>(q / 3, isPlus, rho), in, out);
+    __syncwarp();
+  }
+}
+
 // one pipeline step: issue hop D+1's copies (its neighbour block, from hop 2
-// on, and its link slab), wait for hop D's, compute hop D
-template <typename FT, int S, bool COMP12, int D>
+// on, and its link slab), wait for hop D's, compute hop D.  With hop 7 (spinor
+// buffer 0 is free from then on), the post-hop term's first operand: chi for
+// the A.chi - b.D.psi forms, else piece 0 of the TM-clover FullCloverBlock.
+template <typename FT, int S, bool COMP12, int FAM, bool ACH, int D>
 __device__ __forceinline__ void tw_step(const KArgs<FT> &a, const GeoDev &g, const OpDev<float> &p, const Site &s,
                                         long long obase, const TwinCtx &w, c2 (&acc)[4][3])
 {
+  typedef TwinCfg<FT, S, COMP12> T;
   if constexpr (D < 7) {
     if constexpr (D + 1 >= 2) tw_issue_spinor<FT, S, COMP12, D + 1>(a, w);
     tw_issue_link<FT, S, COMP12, D + 1>(a, w);
+    cp_async_commit();
+    cp_async_wait<1>();
+  } else if constexpr (ACH) {
+    tw_cp<T::SPBB, T::TPG>(w.buf + w.gi * T::SP, a.chi + w.own, w.tig);
+    cp_async_commit();
+    cp_async_wait<1>();
+  } else if constexpr (FAM == FAM_TMCLOV) {
+    tw_issue_fcl_piece<FT, S, COMP12>(a, w, tw_tile<FT, S, COMP12>(w), 0, 0);
     cp_async_commit();
     cp_async_wait<1>();
   } else {
@@ -579,14 +638,14 @@ __device__ __forceinline__ void twin_body(const KArgs<FT> &a, const GeoDev &g, c
   for (int sp = 0; sp < 4; sp++)
 #pragma unroll
     for (int c = 0; c < 3; c++) acc[sp][c].re = acc[sp][c].im = bc(0.f);
-  tw_step<FT, S, COMP12, 0>(a, g, p, s, obase, w, acc);
-  tw_step<FT, S, COMP12, 1>(a, g, p, s, obase, w, acc);
-  tw_step<FT, S, COMP12, 2>(a, g, p, s, obase, w, acc);
-  tw_step<FT, S, COMP12, 3>(a, g, p, s, obase, w, acc);
-  tw_step<FT, S, COMP12, 4>(a, g, p, s, obase, w, acc);
-  tw_step<FT, S, COMP12, 5>(a, g, p, s, obase, w, acc);
-  tw_step<FT, S, COMP12, 6>(a, g, p, s, obase, w, acc);
-  tw_step<FT, S, COMP12, 7>(a, g, p, s, obase, w, acc);
+  tw_step<FT, S, COMP12, FAM, ACH, 0>(a, g, p, s, obase, w, acc);
+  tw_step<FT, S, COMP12, FAM, ACH, 1>(a, g, p, s, obase, w, acc);
+  tw_step<FT, S, COMP12, FAM, ACH, 2>(a, g, p, s, obase, w, acc);
+  tw_step<FT, S, COMP12, FAM, ACH, 3>(a, g, p, s, obase, w, acc);
+  tw_step<FT, S, COMP12, FAM, ACH, 4>(a, g, p, s, obase, w, acc);
+  tw_step<FT, S, COMP12, FAM, ACH, 5>(a, g, p, s, obase, w, acc);
+  tw_step<FT, S, COMP12, FAM, ACH, 6>(a, g, p, s, obase, w, acc);
+  tw_step<FT, S, COMP12, FAM, ACH, 7>(a, g, p, s, obase, w, acc);
 
   // the tile from the table: its chunk addresses are formed here, not held
   // in registers across the hops
@@ -594,11 +653,17 @@ __device__ __forceinline__ void twin_body(const KArgs<FT> &a, const GeoDev &g, c
   const E *clov_tile = a.clov + tl * (FAM == FAM_CLOVER ? 72LL * S : 144LL * S);
   c2 res[4][3];
   if (ACH) {
-    // the hops (subtracted: beta negated by the host), then + A.chi
+    // the hops (subtracted: beta negated by the host), then + A.chi; chi is
+    // in spinor buffer 0 (copied with hop 7)
     c2 ch[4][3];
-    tw_cp<T::SPBB, T::TPG>(w.buf + w.gi * T::SP, a.chi + w.own, w.tig);
-    cp_async_commit();
-    cp_async_wait<0>();
+    if (FAM == FAM_TMCLOV) {
+      // piece 0 of the FullCloverBlock into spinor buffer 1 while chi is read
+      tw_issue_fcl_piece<FT, S, COMP12>(a, w, tl, 0, 1);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
     __syncwarp();
     {
       const unsigned char *grp = w.buf + w.gi * T::SP;
@@ -649,17 +714,8 @@ __device__ __forceinline__ void twin_body(const KArgs<FT> &a, const GeoDev &g, c
                                              rho_of_block<float>(blk, p.isPlus, p.rho), ch, acc);
       __syncwarp();
     } else {
-      // FullCloverBlock halves one at a time
-#pragma unroll
-      for (int blk = 0; blk < 2; blk++) {
-        tw_cp<T::FCB, T::TPG>(w.buf + w.gi * T::FCS, clov_tile + blk * 72LL * S, w.tig);
-        cp_async_commit();
-        cp_async_wait<0>();
-        __syncwarp();
-        dense_apply_tw<FT, S, MODE_ADD, true>(w.buf + w.gi * T::FCS, w.lane, blk,
-                                              rho_of_block<float>(blk, p.isPlus, p.rho), ch, acc);
-        __syncwarp();
-      }
+      // the FullCloverBlock two rows at a time, piece 0 in spinor buffer 1
+      tw_full_clover_pieces<FT, S, COMP12, MODE_ADD, true, 1>(a, w, tl, p.isPlus, p.rho, ch, acc);
     }
 #pragma unroll
     for (int sp = 0; sp < 4; sp++)
@@ -677,15 +733,8 @@ __device__ __forceinline__ void twin_body(const KArgs<FT> &a, const GeoDev &g, c
                                               res);
       __syncwarp();
     } else if (FAM == FAM_TMCLOV) {
-#pragma unroll
-      for (int blk = 0; blk < 2; blk++) {
-        tw_cp<T::FCB, T::TPG>(w.buf + w.gi * T::FCS, clov_tile + blk * 72LL * S, w.tig);
-        cp_async_commit();
-        cp_async_wait<0>();
-        __syncwarp();
-        dense_apply_tw<FT, S, MODE_SET, false>(w.buf + w.gi * T::FCS, w.lane, blk, 0.f, acc, res);
-        __syncwarp();
-      }
+      // two rows at a time, piece 0 (copied with hop 7) in spinor buffer 0
+      tw_full_clover_pieces<FT, S, COMP12, MODE_SET, false, 0>(a, w, tl, p.isPlus, 0.f, acc, res);
     } else if (FAM == FAM_TM) {
       // muinv (1 + sg i mu) acc, sg = -1 on the upper spins for plus
 #pragma unroll
