@@ -50,12 +50,13 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=40,
                     help="steps of the end-to-end pipeline; its drain (one kernel and one device-to-host "
                          "copy) is amortised over them")
-    ap.add_argument("--nrhs", type=int, default=8, help="right-hand sides of --only solve_tm_mrhs")
+    ap.add_argument("--nrhs", type=int, default=8,
+                    help="right-hand sides of --only solve_tm_mrhs / solve_tm_clover_mrhs")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bound of the CPU baseline sample")
     ap.add_argument("--no-extras", action="store_true", help="skip the multi-RHS and solver measurements")
     ap.add_argument("--only", choices=["mrhs", "force", "batch", "solve", "tm", "solve_tm", "solve_tm_clover",
-                                       "solve_tm_mrhs"],
+                                       "solve_tm_mrhs", "solve_tm_clover_mrhs"],
                     help="run one secondary measurement alone (on --dims) and print its JSON line")
     return ap.parse_args()
 
@@ -344,6 +345,42 @@ def bench_solve(dims, dev, nrhs=8, kappa=0.16):
     return out
 
 
+def tm_operators(G, dev, family, kappa, mu, types):
+    """Even-odd operators of the twisted-mass ("tm") or twisted-mass clover
+    ("tm_clover") system of bench_solve_tm on the FP64 geometry G, one per
+    (storage type, torch dtype) in types, from the same seeded fields."""
+    from qphix_b200 import fields, layout
+    from qphix_b200.solver import EvenOddOperator
+    U = fields.random_gauge(G, seed=177, device=dev)
+    gauge = [layout.pack_gauge(G, U, cb, torch.float64) for cb in (0, 1)]
+    del U
+    ops_ = {}
+    if family == "tm":
+        alpha = 1.0 / (2 * kappa)
+        p = dict(coeff_s=0.5, coeff_t_f=0.5, coeff_t_b=0.5, alpha=alpha, mu=mu / alpha,
+                 muinv=alpha / (alpha ** 2 + mu ** 2))
+        for ft, dt in types:
+            ops_[ft] = EvenOddOperator(G.with_(ftype=ft), "tm", gauge=[x.to(dt) for x in gauge], target_cb=1, **p)
+        return ops_
+    mut = 2 * kappa * mu
+    g5 = torch.tensor([1.0, -1.0], dtype=torch.float64, device=dev).reshape(2, 1, 1)
+    eye = torch.eye(6, dtype=torch.complex128, device=dev)
+    clov, clov_dag = [None, None], [None, None]
+    for cb, seed in ((1, 178), (0, 179)):
+        F = fields.random_full_clover(G, seed=seed, device=dev) + 1j * mut * g5 * eye
+        if cb == 0:
+            F = fields.invert_blocks(F)
+        clov[cb] = layout.pack_full_clover(G, F, torch.float64)
+        clov_dag[cb] = layout.pack_full_clover(G, F.conj().transpose(-1, -2), torch.float64)
+        del F
+    p = dict(coeff_s=kappa, coeff_t_f=kappa, coeff_t_b=kappa, rho=0.0)
+    for ft, dt in types:
+        ops_[ft] = EvenOddOperator(G.with_(ftype=ft), "tm_clover", gauge=[x.to(dt) for x in gauge],
+                                   clov=[x.to(dt) for x in clov], clov_dag=[x.to(dt) for x in clov_dag],
+                                   target_cb=1, **p)
+    return ops_
+
+
 def bench_solve_tm(dev, dims=(48, 48, 48, 96), kappa=0.16, mu=0.01, family="tm"):
     """Even-odd twisted-mass (family "tm") or twisted-mass clover ("tm_clover")
     system at 48^3x96, solved for one Gaussian source to |b - Mhat x|/|b| <=
@@ -362,37 +399,10 @@ def bench_solve_tm(dev, dims=(48, 48, 48, 96), kappa=0.16, mu=0.01, family="tm")
     loose tolerance, then three times; the median is reported."""
     from qphix_b200 import fields, layout
     from qphix_b200.lattice import F16N, F32, F64, Geometry
-    from qphix_b200.solver import EvenOddOperator, mixed_solve
+    from qphix_b200.solver import mixed_solve
     G = Geometry(*dims, soalen=8, veclen=8, compress12=True, t_boundary=-1.0, ftype=F64)
-    U = fields.random_gauge(G, seed=177, device=dev)
-    gauge = [layout.pack_gauge(G, U, cb, torch.float64) for cb in (0, 1)]
-    del U
-    ops_ = {}
-    if family == "tm":
-        alpha = 1.0 / (2 * kappa)
-        p = dict(coeff_s=0.5, coeff_t_f=0.5, coeff_t_b=0.5, alpha=alpha, mu=mu / alpha,
-                 muinv=alpha / (alpha ** 2 + mu ** 2))
-        for ft, dt in ((F64, torch.float64), (F32, torch.float32), (F16N, torch.float16)):
-            ops_[ft] = EvenOddOperator(G.with_(ftype=ft), "tm", gauge=[x.to(dt) for x in gauge], target_cb=1, **p)
-    else:
-        mut = 2 * kappa * mu
-        g5 = torch.tensor([1.0, -1.0], dtype=torch.float64, device=dev).reshape(2, 1, 1)
-        eye = torch.eye(6, dtype=torch.complex128, device=dev)
-        clov, clov_dag = [None, None], [None, None]
-        for cb, seed in ((1, 178), (0, 179)):
-            F = fields.random_full_clover(G, seed=seed, device=dev) + 1j * mut * g5 * eye
-            if cb == 0:
-                F = fields.invert_blocks(F)
-            clov[cb] = layout.pack_full_clover(G, F, torch.float64)
-            clov_dag[cb] = layout.pack_full_clover(G, F.conj().transpose(-1, -2), torch.float64)
-            del F
-        p = dict(coeff_s=kappa, coeff_t_f=kappa, coeff_t_b=kappa, rho=0.0)
-        for ft, dt in ((F64, torch.float64), (F32, torch.float32), (F16N, torch.float16)):
-            ops_[ft] = EvenOddOperator(G.with_(ftype=ft), "tm_clover", gauge=[x.to(dt) for x in gauge],
-                                       clov=[x.to(dt) for x in clov], clov_dag=[x.to(dt) for x in clov_dag],
-                                       target_cb=1, **p)
-        del clov, clov_dag
-    del gauge
+    ops_ = tm_operators(G, dev, family, kappa, mu, ((F64, torch.float64), (F32, torch.float32),
+                                                    (F16N, torch.float16)))
     b = layout.pack_spinor(G, fields.random_spinor(G, seed=181, device=dev), torch.float64)
     out = {"lattice": list(dims), "family": family, "kappa": kappa, "mu": mu, "tol": 1e-10,
            "inner_storage": "fp16 + per-site norm (links%s fp16, 12-real)" % (" and clover" if family != "tm" else ""),
@@ -434,37 +444,31 @@ def bench_solve_tm(dev, dims=(48, 48, 48, 96), kappa=0.16, mu=0.01, family="tm")
     return out
 
 
-def bench_solve_tm_mrhs(dev, dims=(48, 48, 48, 96), kappa=0.16, mu=0.01, nrhs=8):
-    """The even-odd twisted-mass system of bench_solve_tm (48^3x96, kappa =
-    0.16, mu = 0.01, 12-real links, SOALEN 8) for nrhs Gaussian sources to
-    |b - Mhat x|/|b| <= 1e-10: (a) the single-RHS FP32 CG corrected in FP64,
-    source by source, against (b) all sources in one FP16-storage multi-RHS
-    CG with FP64 reliable updates (links FP16, each right-hand side scaled
-    to unit norm in its FP16 slot).  Every solution's residual is recomputed
+def bench_solve_tm_mrhs(dev, dims=(48, 48, 48, 96), kappa=0.16, mu=0.01, nrhs=8, family="tm"):
+    """The even-odd twisted-mass (family "tm") or twisted-mass clover
+    ("tm_clover") system of bench_solve_tm (48^3x96, kappa = 0.16, mu = 0.01,
+    12-real links, SOALEN 8) for nrhs Gaussian sources to |b - Mhat x|/|b| <=
+    1e-10: (a) the single-RHS FP32 CG corrected in FP64, source by source,
+    against (b) all sources in one FP16-storage multi-RHS CG with FP64
+    reliable updates (links and clover FP16, each right-hand side scaled to
+    unit norm in its FP16 slot).  Every solution's residual is recomputed
     with the FP64 operator.  One untimed run of each path on a loose
     tolerance, then three timed runs; the median is reported."""
     from qphix_b200 import fields, layout, mrhs
     from qphix_b200.lattice import F16, F32, F64, Geometry
-    from qphix_b200.solver import EvenOddOperator, mixed_solve
+    from qphix_b200.solver import mixed_solve
     G = Geometry(*dims, soalen=8, veclen=8, compress12=True, t_boundary=-1.0, ftype=F64)
-    U = fields.random_gauge(G, seed=177, device=dev)
-    gauge = [layout.pack_gauge(G, U, cb, torch.float64) for cb in (0, 1)]
-    del U
-    alpha = 1.0 / (2 * kappa)
-    p = dict(coeff_s=0.5, coeff_t_f=0.5, coeff_t_b=0.5, alpha=alpha, mu=mu / alpha,
-             muinv=alpha / (alpha ** 2 + mu ** 2))
-    ops_ = {}
-    for ft, dt in ((F64, torch.float64), (F32, torch.float32), (F16, torch.float16)):
-        ops_[ft] = EvenOddOperator(G.with_(ftype=ft), "tm", gauge=[x.to(dt) for x in gauge], target_cb=1, **p)
-    del gauge
+    ops_ = tm_operators(G, dev, family, kappa, mu, ((F64, torch.float64), (F32, torch.float32),
+                                                    (F16, torch.float16)))
     bs = [layout.pack_spinor(G, fields.random_spinor(G, seed=281 + i, device=dev), torch.float64)
           for i in range(nrhs)]
-    out = {"lattice": list(dims), "family": "tm", "kappa": kappa, "mu": mu, "tol": 1e-10, "nrhs": nrhs,
-           "soalen": 8, "inner_storage": "fp16 multi-RHS (links fp16, 12-real)"}
+    out = {"lattice": list(dims), "family": family, "kappa": kappa, "mu": mu, "tol": 1e-10, "nrhs": nrhs,
+           "soalen": 8, "inner_storage": "fp16 multi-RHS (links%s fp16, 12-real)" % (
+               " and clover" if family != "tm" else "")}
     # the FP16 multi-RHS operator's two kernels on this lattice: the plain
-    # twisted-mass dslash (other checkerboard) and the A.chi - b.D.psi form;
-    # bytes per right-hand-side site: psi + out (+ chi) 48 each + 12-real
-    # FP16 links 192 / nrhs
+    # dslash (other checkerboard) and the A.chi - b.D.psi form; bytes per
+    # right-hand-side site: psi + out (+ chi) 48 each + 12-real FP16 links
+    # 192 / nrhs (+ the FullCloverBlock's 288 / nrhs)
     g16 = G.with_(ftype=F16)
     stream = torch.cuda.current_stream()
     peak = measured_peak()[0]
@@ -472,14 +476,22 @@ def bench_solve_tm_mrhs(dev, dims=(48, 48, 48, 96), kappa=0.16, mu=0.01, nrhs=8)
     mp = torch.randn(g16.spinor_elems * nrhs, device=dev).half()
     mc = torch.randn(g16.spinor_elems * nrhs, device=dev).half()
     mo = torch.zeros_like(mp)
-    kw = dict(coeff_s=0.5, coeff_t_f=0.5, coeff_t_b=0.5, mu=mu / alpha, muinv=alpha / (alpha ** 2 + mu ** 2))
+    if family == "tm":
+        alpha = 1.0 / (2 * kappa)
+        kw = dict(coeff_s=0.5, coeff_t_f=0.5, coeff_t_b=0.5, mu=mu / alpha, muinv=alpha / (alpha ** 2 + mu ** 2))
+        fixed, cl_b = {}, 0
+    else:
+        alpha = 1.0
+        kw = dict(coeff_s=kappa, coeff_t_f=kappa, coeff_t_b=kappa)
+        fixed, cl_b = {"clover": op16.keep[1][1]}, 288
     n_rs = g16.vol_cb * nrhs
-    for kern, extra, bps in (("dslash", {}, 96 + 192 / nrhs),
-                             ("achimbdpsi", {"chi": mc, "alpha": alpha}, 144 + 192 / nrhs)):
-        ms = _time(lambda: mrhs.dslash(g16, nrhs, "tm", kern, 1, 0, mp, mo, op16.keep[0][0], **extra, **kw), 20, stream)
-        out["mrhs_tm_%s" % kern] = {"ms": ms, "gbs": bps * n_rs / (ms * 1e-3) / 1e9,
-                                    "frac_of_peak": bps * n_rs / (ms * 1e-3) / 1e9 / peak,
-                                    "bytes_per_rhs_site": bps}
+    for kern, extra, bps in (("dslash", {}, 96 + (192 + cl_b) / nrhs),
+                             ("achimbdpsi", {"chi": mc, "alpha": alpha}, 144 + (192 + cl_b) / nrhs)):
+        ms = _time(lambda: mrhs.dslash(g16, nrhs, family, kern, 1, 0, mp, mo, op16.keep[0][0], **fixed, **extra, **kw),
+                   20, stream)
+        out["mrhs_%s_%s" % (family, kern)] = {"ms": ms, "gbs": bps * n_rs / (ms * 1e-3) / 1e9,
+                                              "frac_of_peak": bps * n_rs / (ms * 1e-3) / 1e9 / peak,
+                                              "bytes_per_rhs_site": bps}
     del mp, mc, mo
     mixed_solve(ops_[F64], ops_[F32], bs[0], tol=1e-4, inner_tol=1e-2)
     mrhs.mixed_solve(ops_[F64], ops_[F16], bs, tol=1e-3, inner_tol=1e-2, solver="cg_reliable")
@@ -911,6 +923,7 @@ def b200_arm(args, world, rank, local):
         extras["solve_tm"] = bench_solve_tm(dev)
         extras["solve_tm_clover"] = bench_solve_tm(dev, family="tm_clover")
         extras["solve_tm_mrhs"] = bench_solve_tm_mrhs(dev)
+        extras["solve_tm_clover_mrhs"] = bench_solve_tm_mrhs(dev, family="tm_clover")
 
     if rank == 0:
         line = {
@@ -959,6 +972,8 @@ def run_only(args):
         r = bench_solve_tm(dev, dims, family="tm_clover")
     elif args.only == "solve_tm_mrhs":
         r = bench_solve_tm_mrhs(dev, dims, nrhs=args.nrhs)
+    elif args.only == "solve_tm_clover_mrhs":
+        r = bench_solve_tm_mrhs(dev, dims, nrhs=args.nrhs, family="tm_clover")
     else:
         r = bench_solve(dims, dev)
     print(json.dumps({"only": args.only, "dims": list(dims), "result": r}))
