@@ -395,8 +395,11 @@ __global__ void __launch_bounds__(128, async_minb<FT, FAM>())
                                       smem[threadIdx.x >> 5]);
 }
 
-// Batched form (see batch_staged_kernel): work unit = one warp's 32 sites of
-// one plane of one item, b.it[k].first and b.total in such warps.
+// Batched form: work unit = one warp's 32 sites of one plane of one item;
+// b.it[k].first and b.total count such warps (each plane padded to whole
+// warps).  The loop is uniform across a warp.  The per-item parameters read
+// through the parameter block take registers: 3 blocks per SM keep it from
+// spilling.
 template <typename FT, int S, bool COMP12, int FAM, bool ACH>
 __global__ void __launch_bounds__(128, 3) batch_async_kernel(const __grid_constant__ BatchDev<FT> b)
 {

@@ -85,19 +85,6 @@ cudaError_t go(const KArgs<FT> &a, const GeoDev &g, const OpDev<typename ftraits
       return cudaGetLastError();
     }
   }
-  // narrow layouts (a spinor component of a block shorter than a sector) with
-  // VECLEN == SOALEN: every field staged through shared memory in 16-byte
-  // vectors
-  if constexpr (!MR && staged_layout<FT, S>()) {
-    const bool al = (((uintptr_t)a.psi | (uintptr_t)a.out | (uintptr_t)a.gauge) % 16 == 0) &&
-                    (!ACH || (uintptr_t)a.chi % 16 == 0) && ((FAM != FAM_CLOVER && FAM != FAM_TMCLOV) || (uintptr_t)a.clov % 16 == 0);
-    if (g.V == S && al) {
-      const long long nb = warp_blocks(g);
-      if (nb > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-      staged_site_kernel<FT, S, COMP12, FAM, ACH><<<(unsigned)nb, kThreads, 0, st>>>(a, g, p);
-      return cudaGetLastError();
-    }
-  }
   // VECLEN known at compile time for the V == S layouts
   if (S >= 4 && g.V == S) site_dslash_kernel<FT, S, COMP12, FAM, ACH, MR, (S >= 4 ? S : 0)><<<grid, kThreads, 0, st>>>(a, g, p);
   else site_dslash_kernel<FT, S, COMP12, FAM, ACH, MR, 0><<<grid, kThreads, 0, st>>>(a, g, p);
@@ -168,9 +155,9 @@ cudaError_t go_unpack(const elem_t<FT> *buf, const elem_t<FT> *gauge, const elem
 template <typename FT, int S, bool COMP12, int FAM, bool ACH>
 cudaError_t go_batch(const BatchDev<FT> &b, bool vfixed, int grid, int block, cudaStream_t st)
 {
-  // async-staged (V == S, S >= 4, 32- or 16-bit) or staged (narrow) kernel,
-  // one warp per 32 sites of a plane
-  if constexpr ((QB_ASYNC && async_layout<FT, S>()) || staged_layout<FT, S>()) {
+  // async-staged kernel (V == S, S >= 4, 32- or 16-bit), one warp per 32
+  // sites of a plane
+  if constexpr (QB_ASYNC && async_layout<FT, S>()) {
     bool al = vfixed;
     for (int k = 0; k < b.n && al; k++) {
       const KArgs<FT> &x = b.it[k].a;
@@ -185,9 +172,7 @@ cudaError_t go_batch(const BatchDev<FT> &b, bool vfixed, int grid, int block, cu
         first += (long long)b.it[k].g.nz * b.it[k].g.nt * ((b.it[k].g.nxh * b.it[k].g.ny + 31) / 32);
       }
       bw.total = first;
-      if constexpr (QB_ASYNC && async_layout<FT, S>())
-        batch_async_kernel<FT, S, COMP12, FAM, ACH><<<grid, block, 0, st>>>(bw);
-      else batch_staged_kernel<FT, S, COMP12, FAM, ACH><<<grid, block, 0, st>>>(bw);
+      batch_async_kernel<FT, S, COMP12, FAM, ACH><<<grid, block, 0, st>>>(bw);
       return cudaGetLastError();
     }
   }

@@ -91,9 +91,11 @@ def test_padding_and_time_edges(cuda):
 @pytest.mark.parametrize("dims,soa,ft", [((8, 6, 4, 4), 4, F32), ((24, 6, 4, 4), 4, F32), ((16, 6, 4, 4), 8, F64),
                                          ((24, 10, 4, 4), 4, F16N), ((48, 2, 4, 4), 8, BF16)])
 def test_staged_layouts_ragged_planes(cuda, dims, soa, ft):
-    """SOALEN 4/8 with VECLEN == SOALEN (the shared-memory staged kernel),
-    including planes whose site count is not a multiple of 32 (idle lanes),
-    padding, and the skipped t hops of a communicated boundary."""
+    """SOALEN 4/8 with VECLEN == SOALEN (the kernels that stage every field
+    through shared memory: async for 32-bit, twin for 16-bit storage; FP64
+    takes the thread-per-site kernel), including planes whose site count is
+    not a multiple of 32 (idle lanes), padding, and the skipped t hops of a
+    communicated boundary."""
     for pad, acc in (((0, 0), None), ((3, 5), [1, 1, 1, 1, 1, 1, 0, 0])):
         g = Geometry(*dims, soalen=soa, veclen=soa, ftype=ft, compress12=True, t_boundary=-1.0,
                      pad_xy=pad[0], pad_xyz=pad[1])
