@@ -397,11 +397,15 @@ __global__ void __launch_bounds__(128, async_minb<FT, FAM>())
 
 // Batched form: work unit = one warp's 32 sites of one plane of one item;
 // b.it[k].first and b.total count such warps (each plane padded to whole
-// warps).  The loop is uniform across a warp.  The per-item parameters read
-// through the parameter block take registers: 3 blocks per SM keep it from
-// spilling.
+// warps).  The loop is uniform across a warp.
+// resident blocks per SM the batched kernel's registers must allow: four
+// (128 registers; the per-item parameters cost a 16-byte spill); five would
+// spill over a kilobyte
+#ifndef QB_BATCH_MINB
+#define QB_BATCH_MINB 4
+#endif
 template <typename FT, int S, bool COMP12, int FAM, bool ACH>
-__global__ void __launch_bounds__(128, 3) batch_async_kernel(const __grid_constant__ BatchDev<FT> b)
+__global__ void __launch_bounds__(128, QB_BATCH_MINB) batch_async_kernel(const __grid_constant__ BatchDev<FT> b)
 {
   __shared__ __align__(16) unsigned char smem[4][AsyncCfg<FT, S, COMP12>::BUF];
   const long long stride = ((long long)gridDim.x * blockDim.x) >> 5;
